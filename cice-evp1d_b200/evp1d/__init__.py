@@ -1,0 +1,235 @@
+"""evp1d -- host-side interface of the B200 EVP-1D sea-ice dynamics solver.
+
+Mirrors the reference's evp1d interface (dmidk/cice-evp1d):
+
+* :func:`set_evp_parameters` -- ``set_evp_parameters`` (src/ice.F90:109-130);
+* :func:`build_index` -- the 1D index space of ``dyn_evp1d_init``
+  (integration/ice_dyn_evp1d.F90:559-589, 743-816);
+* :class:`EVP1D` -- ``dyn_evp1d_init`` / ``dyn_evp1d_run`` /
+  ``dyn_evp1d_finalize`` on the 1D layout, plus the ``lindividual``
+  stress-only / stepu-only loops (src/evp_v2b.F90:127-155).
+
+Every call goes through libevp1d.so (include/evp1d.h); the CUDA kernels are the
+only compute path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import EVP1DError, Fields, Params, check
+
+__all__ = ["EVP1D", "EVP1DError", "Params", "set_evp_parameters",
+           "build_index", "FieldSet", "version"]
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int32)
+
+
+def version() -> str:
+    return _lib.load().evp1d_version().decode()
+
+
+def set_evp_parameters(ndte: int) -> Params:
+    p = Params()
+    _lib.load().evp1d_set_evp_parameters(C.byref(p), int(ndte))
+    return p
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def _as_f64(a, n, name):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.shape != (n,):
+        raise ValueError(f"{name}: expected shape ({n},), got {a.shape}")
+    return a
+
+
+def _as_i32(a, n, name):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    if a.shape != (n,):
+        raise ValueError(f"{name}: expected shape ({n},), got {a.shape}")
+    return a
+
+
+def build_index(mask: np.ndarray, nghost: int = 1):
+    """1D list, halo slots and neighbour vectors of ``mask`` ([nx, ny], True =
+    list point) through the library's native index build.  Returns
+    ``(na, navel, indxti, indxtj, indxtij, {'ee','ne','se','nw','sw','sse'})``
+    with 1-based values."""
+    L = _lib.load()
+    nx, ny = mask.shape
+    m = np.ascontiguousarray(np.asarray(mask, dtype=np.int32).T).reshape(-1)
+    na, navel = C.c_int(), C.c_int()
+    rc = L.evp1d_build_index(nx, ny, nghost, m.ctypes.data_as(_I), 0, 0,
+                             C.byref(na), C.byref(navel), *([None] * 9))
+    if rc != 0 and na.value == 0 and navel.value == 0:
+        check(rc, "evp1d_build_index")
+    n, nv = na.value, navel.value
+    ti = np.zeros(max(n, 1), np.int32)
+    tj = np.zeros(max(n, 1), np.int32)
+    tij = np.zeros(max(nv, 1), np.int32)
+    nb = {k: np.zeros(max(n, 1), np.int32) for k in ("ee", "ne", "se", "nw", "sw", "sse")}
+    rc = L.evp1d_build_index(nx, ny, nghost, m.ctypes.data_as(_I), n, nv,
+                             C.byref(na), C.byref(navel),
+                             ti.ctypes.data_as(_I), tj.ctypes.data_as(_I),
+                             tij.ctypes.data_as(_I),
+                             *[nb[k].ctypes.data_as(_I) for k in ("ee", "ne", "se", "nw", "sw", "sse")])
+    check(rc, "evp1d_build_index")
+    return n, nv, ti[:n], tj[:n], tij[:nv], {k: v[:n] for k, v in nb.items()}
+
+
+class FieldSet:
+    """Host arrays of one dyn_evp1d_run call (evp1d_fields), kept alive while
+    the ctypes struct points at them.  Arrays are updated in place by
+    :meth:`EVP1D.run` / :meth:`EVP1D.download`."""
+
+    DYN = ("strength", "Cw", "aiu", "uocn", "vocn", "waterx", "watery",
+           "forcex", "forcey", "umassdti", "fm", "Tbu")
+
+    def __init__(self, na: int, navel: int, *, skipT, skipU, stress, uvel,
+                 vvel, strintx, strinty, Cb, uvel_init=None, vvel_init=None,
+                 want_str: bool = False, **dyn):
+        self.na, self.navel = na, navel
+        self.skipT = _as_i32(skipT, na, "skipT")
+        self.skipU = _as_i32(skipU, na, "skipU")
+        stress = np.ascontiguousarray(stress, dtype=np.float64)
+        if stress.shape != (12, na):
+            raise ValueError(f"stress: expected (12, {na}), got {stress.shape}")
+        self.stress = stress
+        self.dyn = {k: _as_f64(dyn[k], na, k) for k in self.DYN}
+        self.uvel = _as_f64(uvel, navel, "uvel")
+        self.vvel = _as_f64(vvel, navel, "vvel")
+        self.strintx = _as_f64(strintx, na, "strintx")
+        self.strinty = _as_f64(strinty, na, "strinty")
+        self.Cb = _as_f64(Cb, na, "Cb")
+        self.uvel_init = None if uvel_init is None else _as_f64(uvel_init, na, "uvel_init")
+        self.vvel_init = None if vvel_init is None else _as_f64(vvel_init, na, "vvel_init")
+        self.str = np.zeros((8, navel)) if want_str else None
+        f = Fields()
+        f.skipT = self.skipT.ctypes.data_as(_I)
+        f.skipU = self.skipU.ctypes.data_as(_I)
+        for k in range(12):
+            f.stress[k] = self.stress[k].ctypes.data_as(_D)
+        for k in self.DYN:
+            setattr(f, k, _d(self.dyn[k]))
+        f.uvel_init = _d(self.uvel_init)
+        f.vvel_init = _d(self.vvel_init)
+        f.uvel, f.vvel = _d(self.uvel), _d(self.vvel)
+        f.strintx, f.strinty, f.Cb = _d(self.strintx), _d(self.strinty), _d(self.Cb)
+        for k in range(8):
+            f.str[k] = self.str[k].ctypes.data_as(_D) if self.str is not None else None
+        self.c = f
+
+    @classmethod
+    def from_problem(cls, prob, want_str: bool = False, copy: bool = True,
+                     explicit_init: bool = False) -> "FieldSet":
+        """Fields of a :class:`evp1d.synth.Problem1D` (copied by default)."""
+        cp = (lambda a: np.array(a, copy=True)) if copy else (lambda a: a)
+        dyn = {k: cp(prob.f[k]) for k in cls.DYN}
+        return cls(prob.na, prob.navel, skipT=prob.skipT, skipU=prob.skipU,
+                   stress=cp(prob.stress), uvel=cp(prob.uvel),
+                   vvel=cp(prob.vvel), strintx=cp(prob.strintx),
+                   strinty=cp(prob.strinty), Cb=cp(prob.Cb),
+                   uvel_init=prob.f["uvel_init"] if explicit_init else None,
+                   vvel_init=prob.f["vvel_init"] if explicit_init else None,
+                   want_str=want_str, **dyn)
+
+
+class EVP1D:
+    """One 1D EVP problem resident on a GPU (dyn_evp1d_init ... finalize)."""
+
+    def __init__(self, na: int, navel: int, *, ee, ne, se, nw, sw, sse, dxT,
+                 dyT, HTE, HTN, HTEm1, HTNm1, uarear, params: Params = None,
+                 ndte: int = None, device: int = 0):
+        L = _lib.load()
+        self._L = L
+        self.na, self.navel = int(na), int(navel)
+        if params is None:
+            if ndte is None:
+                raise ValueError("give params or ndte")
+            params = set_evp_parameters(ndte)
+        self.params = params
+        idx = [_as_i32(a, na, n) for a, n in
+               ((ee, "ee"), (ne, "ne"), (se, "se"), (nw, "nw"), (sw, "sw"), (sse, "sse"))]
+        geo = [_as_f64(a, na, n) for a, n in
+               ((dxT, "dxT"), (dyT, "dyT"), (HTE, "HTE"), (HTN, "HTN"),
+                (HTEm1, "HTEm1"), (HTNm1, "HTNm1"), (uarear, "uarear"))]
+        h = C.c_void_p()
+        rc = L.evp1d_init(C.byref(h), self.na, self.navel,
+                          *[a.ctypes.data_as(_I) for a in idx],
+                          *[a.ctypes.data_as(_D) for a in geo],
+                          C.byref(params), int(device))
+        check(rc, "evp1d_init")
+        self.h = h
+
+    @classmethod
+    def from_problem(cls, prob, ndte: int = None, params: Params = None,
+                     device: int = 0) -> "EVP1D":
+        f = prob.f
+        return cls(prob.na, prob.navel, **prob.idx, dxT=f["dxT"], dyT=f["dyT"],
+                   HTE=f["HTE"], HTN=f["HTN"], HTEm1=f["HTEm1"],
+                   HTNm1=f["HTNm1"], uarear=f["uarear"], params=params,
+                   ndte=ndte if ndte is not None else prob.ndte, device=device)
+
+    # -- dyn_evp1d_run -----------------------------------------------------
+    def run(self, ndte: int, fields: FieldSet) -> FieldSet:
+        check(self._L.evp1d_run(self.h, int(ndte), C.byref(fields.c)), "evp1d_run")
+        return fields
+
+    def upload(self, fields: FieldSet) -> None:
+        check(self._L.evp1d_upload(self.h, C.byref(fields.c)), "evp1d_upload")
+
+    def subcycles(self, ndte: int) -> None:
+        check(self._L.evp1d_subcycles(self.h, int(ndte)), "evp1d_subcycles")
+
+    def download(self, fields: FieldSet) -> FieldSet:
+        check(self._L.evp1d_download(self.h, C.byref(fields.c)), "evp1d_download")
+        return fields
+
+    # -- lindividual -------------------------------------------------------
+    def stress_only(self, n: int) -> None:
+        check(self._L.evp1d_stress_only(self.h, int(n)), "evp1d_stress_only")
+
+    def stepu_only(self, n: int) -> None:
+        check(self._L.evp1d_stepu_only(self.h, int(n)), "evp1d_stepu_only")
+
+    def set_params(self, params: Params) -> None:
+        check(self._L.evp1d_set_params(self.h, C.byref(params)), "evp1d_set_params")
+        self.params = params
+
+    def synchronize(self) -> None:
+        check(self._L.evp1d_synchronize(self.h), "evp1d_synchronize")
+
+    @property
+    def path(self) -> str:
+        """Name of the kernel path the library runs."""
+        return "two-kernel"
+
+    @property
+    def stream(self) -> int:
+        return self._L.evp1d_stream(self.h) or 0
+
+    def launch_count(self, reset: bool = False) -> int:
+        return int(self._L.evp1d_launch_count(self.h, 1 if reset else 0))
+
+    def finalize(self) -> None:
+        if getattr(self, "h", None):
+            check(self._L.evp1d_finalize(self.h), "evp1d_finalize")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.finalize()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.finalize()

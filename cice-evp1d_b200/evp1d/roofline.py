@@ -1,0 +1,58 @@
+"""Roofline bookkeeping for the EVP-1D kernels.
+
+Algorithmic bytes are the bytes a kernel path must move between HBM and the
+SMs per ice-point-subcycle under its own data flow, with every array touched
+once and neighbour gathers served from cache:
+
+* ``two-kernel`` -- the reference's data contract (src/bench_v2b.F90:62-549):
+  21 per-point input doubles (stress: dxT, dyT, HTE, HTN, HTEm1, HTNm1,
+  strength; stepu: Cw, aiu, uocn, vocn, waterx, watery, forcex, forcey,
+  umassdti, fm, uarear, Tbu, uvel_init, vvel_init), u/v read + write (4),
+  12 stresses read + write (24), str1..8 written by stress and read by stepu
+  (16), strintx/strinty/Cb written (3): 68 doubles = 544 B, plus 6 int32
+  neighbour indices (24 B) and two 4-byte skip flags (8 B) = 576 B.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+BYTES_PER_POINT_SUBCYCLE = {
+    "two-kernel": 576,
+}
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def per_point_subcycle(path: str) -> int:
+    return BYTES_PER_POINT_SUBCYCLE[path]
+
+
+def hbm_peak(root: str):
+    """Measured HBM copy bandwidth (GB/s) and where it came from."""
+    p = os.path.join(root, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def host_bytes(pr) -> tuple:
+    """Bytes copied host->device and device->host by one evp1d_run call with
+    uvel_init/vvel_init defaulted and str not requested."""
+    na, navel = pr.na, pr.navel
+    h2d = na * 1 + 8 * na * (12 + 12 + 3) + 8 * navel * 2
+    d2h = 8 * na * (12 + 2 + 3)
+    return h2d, d2h
+
+
+def measured_traffic(root: str, path: str, config: str):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    p = os.path.join(root, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)[path][config]["dram_bytes_per_launch"]
+    except Exception:
+        return None

@@ -1,0 +1,170 @@
+/*
+ * evp1d.h -- C-ABI of the B200 (sm_100a) EVP-1D sea-ice dynamics solver.
+ *
+ * Drop-in for the ndte-subcycle loop of CICE's 1D EVP solver as restructured
+ * by dmidk/cice-evp1d: the `stress` and `stepu` kernels of module `bench`
+ * (src/bench_v2b.F90:62-312, 444-549) called ndte times from
+ * dyn_evp1d_run (integration/ice_dyn_evp1d.F90:188-207).
+ *
+ * Conventions
+ *  - Plain C types only: int32_t indices, double fields, host pointers unless
+ *    a function says "device".
+ *  - 1D layout as in the reference: `na` list points, `navel >= na` slots
+ *    where slots na+1..navel are halo points (outside the list).  Neighbour
+ *    vectors are 1-BASED, exactly as the Fortran module stores them
+ *    (integration/ice_dyn_evp1d.F90:792-797).  Per-point fields have length
+ *    na; uvel, vvel and str1..str8 have length navel.
+ *  - Every function returns EVP1D_OK (0) or a negative EVP1D_ERR_* code;
+ *    evp1d_last_error() gives a message.  Nothing aborts the process (the
+ *    reference calls `stop`, integration/ice_dyn_evp1d.F90:394-460,1039).
+ *  - A handle owns its device buffers and one CUDA stream.  It is not
+ *    thread-safe; use one handle per host thread.
+ *  - All arithmetic is IEEE FP64 in the reference's operation order with no
+ *    FMA contraction: results are bit-identical to the reference's f0/f1
+ *    (-fp-model precise -no-fma) builds on the same input.
+ */
+#ifndef EVP1D_H
+#define EVP1D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EVP1D_OK 0
+#define EVP1D_ERR_INVALID_ARG (-1) /* NULL pointer, bad size, bad ndte       */
+#define EVP1D_ERR_INDEX (-2)       /* neighbour index outside 1..navel, or a
+                                      list point that is not its own slot   */
+#define EVP1D_ERR_CUDA (-3)        /* a CUDA runtime call failed            */
+#define EVP1D_ERR_NOMEM (-4)       /* device or pinned allocation failed    */
+#define EVP1D_ERR_TIMEOUT (-5)     /* a bounded device-side wait ran out    */
+#define EVP1D_ERR_NO_DEVICE (-6)   /* no CUDA device of compute 10.x        */
+#define EVP1D_ERR_STATE (-7)       /* call out of order (e.g. no upload)    */
+
+/* EVP parameters.  Field meanings follow ice_dyn_shared (src/ice.F90:80-130)
+ * including the values read from the input file (src/vars.F90:2116). */
+typedef struct evp1d_params {
+  double arlx1i;      /* 1 / (2 * elasticDamp * ndte)                   */
+  double denom1;      /* 1 / (1 + arlx1i)                               */
+  double brlx;        /* ndte                                           */
+  double capping;     /* 1: capped viscosities                          */
+  double e_factor;    /* e_yieldcurve^2 / e_plasticpot^4                */
+  double epp2i;       /* 1 / e_plasticpot^2                             */
+  double deltaminEVP; /* minimum Delta (1e-8)                           */
+  double revp;        /* 0 classic EVP, 1 revised EVP                   */
+  double Ktens;       /* tensile strength factor                        */
+  double u0;          /* basal-stress residual speed (5e-5 m/s)         */
+  double cosw, sinw;  /* ocean turning angle                            */
+  double rhow;        /* sea-water density (1026 kg/m^3)                */
+} evp1d_params;
+
+/* Per-call fields of dyn_evp1d_run in the 1D layout (host pointers).
+ * Replaces the argument lists of stress/stepu (src/bench_v2b.F90:62-68,
+ * 444-458) and the L_* arrays of dyn_evp1d_run
+ * (integration/ice_dyn_evp1d.F90:115-138).  in = read, inout = read and
+ * written back, out = written. */
+typedef struct evp1d_fields {
+  const int32_t *skipT;     /* in  [na]  nonzero: not an ice T point      */
+  const int32_t *skipU;     /* in  [na]  nonzero: not an ice U point      */
+  double *stress[12];       /* inout [na] stressp_1..4, stressm_1..4,
+                                          stress12_1..4                  */
+  const double *strength;   /* in  [na]                                   */
+  const double *Cw;         /* in  [na]  cdn_ocn                          */
+  const double *aiu;        /* in  [na]                                   */
+  const double *uocn, *vocn;      /* in [na]                              */
+  const double *waterx, *watery;  /* in [na]                              */
+  const double *forcex, *forcey;  /* in [na]                              */
+  const double *umassdti;   /* in  [na]                                   */
+  const double *fm;         /* in  [na]                                   */
+  const double *Tbu;        /* in  [na]                                   */
+  const double *uvel_init;  /* in  [na]  NULL: uvel at the start of the call
+                                         (src/vars.F90:2119-2120)         */
+  const double *vvel_init;  /* in  [na]  NULL: vvel at the start          */
+  double *uvel, *vvel;      /* inout [navel]; list slots 1..na are updated,
+                               halo slots na+1..navel are read as given and
+                               never written (the adapter passes 0 there,
+                               integration/ice_dyn_evp1d.F90:880-881)      */
+  double *strintx, *strinty;/* inout [na]; written at ice U points        */
+  double *Cb;               /* inout [na]; written at ice U points        */
+  double *str[8];           /* out [navel] str1..str8 of the last subcycle,
+                               each may be NULL (not returned)            */
+} evp1d_fields;
+
+typedef struct evp1d_handle evp1d_t;
+
+/* set_evp_parameters for a given ndte (src/ice.F90:109-130). */
+void evp1d_set_evp_parameters(evp1d_params *p, int ndte);
+
+/* Set up the static part of the 1D problem on `device`.
+ * Replaces the index/geometry part of dyn_evp1d_init
+ * (integration/ice_dyn_evp1d.F90:65-112, 743-816): neighbour vectors (1-based,
+ * [na]) and the static per-point geometry ([na]).  Indices are validated on
+ * the host (EVP1D_ERR_INDEX) so that no device access can leave its buffer.
+ * na = 0 is allowed (every run is then a no-op). */
+int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
+               const int32_t *ne, const int32_t *se, const int32_t *nw,
+               const int32_t *sw, const int32_t *sse, const double *dxT,
+               const double *dyT, const double *HTE, const double *HTN,
+               const double *HTEm1, const double *HTNm1, const double *uarear,
+               const evp1d_params *params, int device);
+
+/* Release the handle and its device buffers (dyn_evp1d_finalize,
+ * integration/ice_dyn_evp1d.F90:326-331).  NULL is a no-op. */
+int evp1d_finalize(evp1d_t *handle);
+
+/* Replace the EVP parameters (e.g. after a change of ndte). */
+int evp1d_set_params(evp1d_t *handle, const evp1d_params *params);
+
+/* One call of the subcycle loop with host buffers: upload the fields, run
+ * ndte x {stress; stepu} on the GPU, download the results.  Replaces
+ * integration/ice_dyn_evp1d.F90:179-225 and src/evp_v2b.F90:91-110. */
+int evp1d_run(evp1d_t *handle, int ndte, const evp1d_fields *io);
+
+/* The same call split in three, for callers that keep the state on the GPU
+ * between calls or time the device work alone. */
+int evp1d_upload(evp1d_t *handle, const evp1d_fields *io);
+int evp1d_subcycles(evp1d_t *handle, int ndte); /* device-resident */
+int evp1d_download(evp1d_t *handle, const evp1d_fields *io);
+
+/* lindividual-style loops on the device-resident state
+ * (src/evp_v2b.F90:127-155): n x stress alone, n x stepu alone.  stepu_only
+ * reads str1..str8 left by the last stress pass. */
+int evp1d_stress_only(evp1d_t *handle, int n);
+int evp1d_stepu_only(evp1d_t *handle, int n);
+
+/* Wait for the handle's stream. */
+int evp1d_synchronize(evp1d_t *handle);
+
+/* The handle's CUDA stream (a cudaStream_t), for event timing by callers. */
+void *evp1d_stream(evp1d_t *handle);
+
+/* Number of kernel launches issued on the handle's stream since the last
+ * reset (pass reset != 0 to zero the counter). */
+long long evp1d_launch_count(evp1d_t *handle, int reset);
+
+/* Message of the last error on this host thread ("" if none). */
+const char *evp1d_last_error(void);
+
+/* Library version string. */
+const char *evp1d_version(void);
+
+/* ----------------------------------------------------------------------------
+ * Index build on the host, no GPU needed.
+ * calc_2d_indices_init + calc_navel + convert_2d_1d_init
+ * (integration/ice_dyn_evp1d.F90:559-589, 743-797, 1000-1087).
+ * mask: [nx*ny] column-major (i fastest), nonzero = point in the 1D list.
+ * Outputs are caller-allocated: indxti, indxtj [cap_na]; indxtij [cap_navel];
+ * ee..sse [cap_na] 1-based.  Returns EVP1D_ERR_INVALID_ARG when a capacity is
+ * too small (*na_out / *navel_out then hold the sizes needed).
+ * -------------------------------------------------------------------------- */
+int evp1d_build_index(int nx, int ny, int nghost, const int32_t *mask,
+                      int cap_na, int cap_navel, int *na_out, int *navel_out,
+                      int32_t *indxti, int32_t *indxtj, int32_t *indxtij,
+                      int32_t *ee, int32_t *ne, int32_t *se, int32_t *nw,
+                      int32_t *sw, int32_t *sse);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EVP1D_H */

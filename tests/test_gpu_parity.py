@@ -1,0 +1,194 @@
+"""GPU parity: the CUDA path through the C-ABI against the oracle, bit for bit.
+
+The tolerance is zero: with -fmad=false every output must be bitwise equal
+to the oracle's no-FMA CPU restatement (the reference's f0/f1 semantics), and
+the two md5-compared output files (src/vars.F90:2233-2304) must hash equal.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import evp1d
+from evp1d import synth
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_run(pr, ndte, params=None, want_str=True, explicit_init=False, calls=1):
+    fs = evp1d.FieldSet.from_problem(pr, want_str=want_str, explicit_init=explicit_init)
+    with evp1d.EVP1D.from_problem(pr, ndte=ndte, params=params) as s:
+        for _ in range(calls):
+            s.run(ndte, fs)
+    return fs
+
+
+def oracle_run(oracle_mod, pr, ndte, params=None):
+    p = params if params is not None else oracle_mod.params(ndte)
+    op = oracle_mod.OracleParams(**{k: getattr(p, k) for k in evp1d._lib.PARAM_FIELDS})
+    return oracle_mod.run_1d(pr, ndte, p=op)
+
+
+def assert_same(fs, st, pr, check_str=True):
+    na = pr.na
+    for name, a, b in (("stress", fs.stress, st.stress), ("uvel", fs.uvel[:na], st.uvel[:na]),
+                       ("vvel", fs.vvel[:na], st.vvel[:na]),
+                       ("strintx", fs.strintx, st.strintx), ("strinty", fs.strinty, st.strinty),
+                       ("Cb", fs.Cb, st.Cb)):
+        assert np.array_equal(np.asarray(a).view(np.int64), np.asarray(b).view(np.int64)), \
+            f"{name}: {helpers.first_mismatch(a, b)}"
+    if check_str and fs.str is not None:
+        assert np.array_equal(fs.str.view(np.int64), st.str[:, : pr.navel].view(np.int64)), \
+            "str: " + helpers.first_mismatch(fs.str, st.str[:, : pr.navel])
+    f = helpers.output_files(fs.stress, fs.strintx, fs.strinty, fs.uvel, fs.vvel, pr.skipU)
+    g = helpers.output_files(st.stress, st.strintx, st.strinty, st.uvel, st.vvel, pr.skipU)
+    assert helpers.md5(f[0]) == helpers.md5(g[0])
+    assert helpers.md5(f[1]) == helpers.md5(g[1])
+
+
+@pytest.mark.parametrize("curvilinear", [False, True])
+@pytest.mark.parametrize("nx,ny,seed,ndte", [(60, 40, 3, 20), (131, 77, 9, 13)])
+def test_small_grids_bitwise(oracle_mod, nx, ny, seed, ndte, curvilinear):
+    pr = synth.to_1d(synth.make_grid(nx, ny, seed=seed, ndte=ndte, curvilinear=curvilinear))
+    assert_same(gpu_run(pr, ndte), oracle_run(oracle_mod, pr, ndte), pr)
+
+
+def test_cfg1_full_md5(oracle_mod):
+    """400 x 300 synthetic grid, ndte = 120: md5-identical output files."""
+    pr = synth.make_problem("cfg1")
+    assert_same(gpu_run(pr, pr.ndte, want_str=False), oracle_run(oracle_mod, pr, pr.ndte),
+                pr, check_str=False)
+
+
+def test_two_calls_carry_state(oracle_mod):
+    """Two dyn_evp1d_run calls in a row: the second starts from the first's
+    stresses and velocities."""
+    pr = synth.make_problem("cfg1", nx=80, ny=60, ndte=10)
+    fs = gpu_run(pr, 10, calls=2)
+    st = oracle_run(oracle_mod, pr, 10)
+    pr2 = pr.copy()
+    pr2.stress[:] = st.stress
+    pr2.uvel[:] = st.uvel[: pr.navel]
+    pr2.vvel[:] = st.vvel[: pr.navel]
+    pr2.strintx[:], pr2.strinty[:], pr2.Cb[:] = st.strintx, st.strinty, st.Cb
+    assert_same(fs, oracle_run(oracle_mod, pr2, 10), pr2)
+
+
+def test_standalone_closed_form():
+    """Integration smoke-test state with strength = 0: stress = stress0 *
+    denom1**ndte exactly."""
+    ndte = 4
+    pr = helpers.standalone_problem(ndte=ndte)
+    fs = gpu_run(pr, ndte)
+    p = evp1d.set_evp_parameters(ndte)
+    want = pr.stress.copy()
+    for _ in range(ndte):
+        want = want * p.denom1
+    assert np.array_equal(fs.stress, want)
+    assert np.all(fs.Cb == 0)
+
+
+def test_standalone_with_strength(oracle_mod):
+    pr = helpers.standalone_problem(ndte=3, strength=2.5e4)
+    assert_same(gpu_run(pr, 3), oracle_run(oracle_mod, pr, 3), pr)
+
+
+def test_every_parameter_path(oracle_mod):
+    """Revised EVP with explicit uvel_init, basal stress, turning angle,
+    tensile strength and capping = 0: every term of stress/stepu is live."""
+    g = synth.make_grid(70, 50, seed=21, ndte=15, curvilinear=True)
+    rng = np.random.default_rng(5)
+    g.f["Tbu"] = np.asfortranarray(rng.uniform(0.0, 5.0, g.f["Tbu"].shape))
+    g.f["fm"] = np.asfortranarray(g.f["fm"] * np.where(rng.random(g.f["fm"].shape) < 0.3, -1, 1))
+    pr = synth.to_1d(g)
+    pr.f["uvel_init"] = pr.f["uvel_init"] + rng.normal(0, 0.01, pr.na)
+    p = evp1d.set_evp_parameters(15)
+    p.revp, p.Ktens, p.capping = 1.0, 0.2, 0.0
+    p.cosw, p.sinw = np.cos(0.4), np.sin(0.4)
+    fs = gpu_run(pr, 15, params=p, explicit_init=True)
+    assert_same(fs, oracle_run(oracle_mod, pr, 15, params=p), pr)
+    assert np.any(fs.Cb != 0)
+
+
+def test_halo_velocity_read_as_given(oracle_mod):
+    """Halo slots of uvel/vvel are inputs (src/vars.F90:2108 reads
+    uvel(1:navel)); nonzero halo values feed the stress gathers."""
+    pr = synth.make_problem("cfg1", nx=50, ny=40, ndte=6)
+    rng = np.random.default_rng(2)
+    pr.uvel[pr.na:] = rng.normal(0, 0.05, pr.navel - pr.na)
+    pr.vvel[pr.na:] = rng.normal(0, 0.05, pr.navel - pr.na)
+    fs = gpu_run(pr, 6)
+    assert_same(fs, oracle_run(oracle_mod, pr, 6), pr)
+    assert np.array_equal(fs.uvel[pr.na:], pr.uvel[pr.na:])
+
+
+@pytest.mark.parametrize("which", ["allT", "allU", "none"])
+def test_skip_patterns(oracle_mod, which):
+    pr = synth.make_problem("cfg1", nx=40, ny=30, ndte=5)
+    if which == "allT":
+        pr.skipT[:] = 1
+    elif which == "allU":
+        pr.skipU[:] = 1
+    else:
+        pr.skipT[:] = 0
+        pr.skipU[:] = 0
+    assert_same(gpu_run(pr, 5), oracle_run(oracle_mod, pr, 5), pr)
+
+
+def test_empty_problem():
+    p = evp1d.set_evp_parameters(5)
+    z = np.zeros(0, np.int32)
+    zd = np.zeros(0)
+    with evp1d.EVP1D(0, 0, ee=z, ne=z, se=z, nw=z, sw=z, sse=z, dxT=zd, dyT=zd,
+                     HTE=zd, HTN=zd, HTEm1=zd, HTNm1=zd, uarear=zd, params=p) as s:
+        fs = evp1d.FieldSet(0, 0, skipT=z, skipU=z, stress=np.zeros((12, 0)),
+                            uvel=zd, vvel=zd, strintx=zd, strinty=zd, Cb=zd,
+                            **{k: zd for k in evp1d.FieldSet.DYN})
+        s.run(5, fs)
+        s.stress_only(3)
+        s.stepu_only(3)
+
+
+def test_lindividual_loops(oracle_mod):
+    """stress alone n times, then stepu alone n times (src/evp_v2b.F90:127-155)."""
+    pr = synth.make_problem("cfg1", nx=60, ny=45, ndte=4)
+    fs = evp1d.FieldSet.from_problem(pr, want_str=True)
+    st = oracle_mod.State1D(pr)
+    op = oracle_mod.params(4)
+    with evp1d.EVP1D.from_problem(pr, ndte=4) as s:
+        s.upload(fs)
+        s.stress_only(3)
+        s.stepu_only(2)
+        s.download(fs)
+    oracle_mod.run_1d(pr, 3, p=op, mode="stress", state=st)
+    oracle_mod.run_1d(pr, 2, p=op, mode="stepu", state=st)
+    assert_same(fs, st, pr)
+
+
+def test_error_paths_on_device():
+    pr = synth.make_problem("cfg1", nx=30, ny=20, ndte=3)
+    with evp1d.EVP1D.from_problem(pr, ndte=3) as s:
+        with pytest.raises(evp1d.EVP1DError) as e:
+            s.subcycles(3)  # nothing uploaded
+        assert e.value.code == -7
+        with pytest.raises(evp1d.EVP1DError) as e:
+            s.subcycles(-1)
+        assert e.value.code == -1
+        fs = evp1d.FieldSet.from_problem(pr)
+        fs.c.strength = None
+        with pytest.raises(evp1d.EVP1DError) as e:
+            s.upload(fs)
+        assert e.value.code == -1
+    with pytest.raises(evp1d.EVP1DError) as e:
+        evp1d.EVP1D.from_problem(pr, ndte=3, device=4096)
+    assert e.value.code == -1
+
+
+def test_launch_count_is_native():
+    pr = synth.make_problem("cfg1", nx=30, ny=20, ndte=7)
+    fs = evp1d.FieldSet.from_problem(pr)
+    with evp1d.EVP1D.from_problem(pr, ndte=7) as s:
+        s.launch_count(reset=True)
+        s.run(7, fs)
+        assert s.launch_count() > 0
