@@ -2,15 +2,16 @@
 // device movement and the graph-launched subcycle loop.
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "evp1d.h"
-#include "evp_kernels.cuh"
 #include "evp_internal.h"
 
 using evp::DevState;
+using evp::DeviceProblem;
 using evp::Params;
 
 namespace {
@@ -42,9 +43,9 @@ namespace {
                   "%s: %s", #x, cudaGetErrorString(e_));                   \
   } while (0)
 
-#define CHECK(x) \
-  do {           \
-    int rc_ = (x); \
+#define CHECK(x)                    \
+  do {                              \
+    int rc_ = (x);                  \
     if (rc_ != EVP1D_OK) return rc_; \
   } while (0)
 
@@ -66,71 +67,85 @@ Params to_params(const evp1d_params &q) {
   return p;
 }
 
-size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
-
-// Number of subcycles captured in one CUDA graph.
+// Subcycles per captured CUDA graph.  Even, so that a graph leaves the
+// ping-pong parity unchanged.
 constexpr int kGraphChunk = 50;
 
 }  // namespace
 
+// Kernel paths of the fused subcycle.
+enum { kPathTma = 0, kPathFused = 1 };
+
 struct evp1d_handle {
-  int device = 0;
-  cudaStream_t stream = nullptr;
+  DeviceProblem d;
   Params p{};
-  DevState s{};
-  void *arena = nullptr;
-  size_t arena_bytes = 0;
+  int path = kPathTma;
   bool uploaded = false;
-  bool have_str = false;  // str holds the result of a stress pass
   long long launches = 0;
-  cudaGraphExec_t graph = nullptr;
-  int graph_n = 0;
-  std::vector<uint8_t> flags_host;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // by starting buffer
 };
 
 namespace {
 
 int select_device(evp1d_t *h) {
-  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaSetDevice(h->d.device));
   return EVP1D_OK;
 }
 
-void drop_graph(evp1d_t *h) {
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  h->graph = nullptr;
-  h->graph_n = 0;
-}
-
-// Launch `n` subcycles of {stress; stepu} directly.
-void launch_subcycles_direct(evp1d_t *h, int n) {
-  for (int k = 0; k < n; k++) {
-    evp::launch_stress(h->s, h->p, h->stream);
-    evp::launch_stepu(h->s, h->p, h->stream);
+void drop_graphs(evp1d_t *h) {
+  for (int k = 0; k < 2; k++) {
+    if (h->graph[k]) cudaGraphExecDestroy(h->graph[k]);
+    h->graph[k] = nullptr;
   }
-  h->launches += 2LL * n;
 }
 
-int build_graph(evp1d_t *h, int n) {
-  drop_graph(h);
+// One subcycle from buffer `from` into the other one.
+void launch_sub(evp1d_t *h, int from, bool last) {
+  if (h->path == kPathTma)
+    evp::launch_tma(evp::problem_tma_args(h->d, from), h->p, last, h->d.nctas, h->d.stream);
+  else
+    evp::launch_fused(evp::problem_fused_args(h->d, from), h->p, last, h->d.stream);
+}
+
+// A bounded device-side wait that ran out leaves a code in the error word.
+int check_device_error(evp1d_t *h) {
+  int code = 0;
+  CHECK(evp::problem_take_error(&h->d, &code));
+  if (code)
+    return fail(EVP1D_ERR_TIMEOUT,
+                "a bounded device wait ran out (code %d: 1 consumer, 2 producer, "
+                "3 drain); the results of this call are not valid", code);
+  return EVP1D_OK;
+}
+
+// Capture kGraphChunk non-final fused subcycles starting from buffer `from`.
+int build_graph(evp1d_t *h, int from) {
+  cudaStream_t st = h->d.stream;
   cudaGraph_t g = nullptr;
-  CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  for (int k = 0; k < n; k++) {
-    evp::launch_stress(h->s, h->p, h->stream);
-    evp::launch_stepu(h->s, h->p, h->stream);
+  CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  int b = from;
+  for (int k = 0; k < kGraphChunk; k++) {
+    launch_sub(h, b, false);
+    b = 1 - b;
   }
-  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  cudaError_t e = cudaStreamEndCapture(st, &g);
   if (e != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
     return fail(EVP1D_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
   }
-  e = cudaGraphInstantiate(&h->graph, g, 0);
+  e = cudaGraphInstantiate(&h->graph[from], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
-    h->graph = nullptr;
+    h->graph[from] = nullptr;
     return fail(EVP1D_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
   }
-  h->graph_n = n;
   return EVP1D_OK;
+}
+
+bool nonnull_all(const void *const *p, int n) {
+  for (int k = 0; k < n; k++)
+    if (!p[k]) return false;
+  return true;
 }
 
 }  // namespace
@@ -139,7 +154,9 @@ extern "C" {
 
 const char *evp1d_last_error(void) { return g_err.c_str(); }
 
-const char *evp1d_version(void) { return "evp1d-b200 0.1 (sm_100a, fp64)"; }
+const char *evp1d_version(void) {
+  return "evp1d-b200 0.2 (sm_100a, fp64, fused tile solver)";
+}
 
 void evp1d_set_evp_parameters(evp1d_params *p, int ndte) {
   // set_evp_parameters (src/ice.F90:109-130) with the fixed values of
@@ -179,10 +196,10 @@ int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
   const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
   const double *geo[7] = {dxT, dyT, HTE, HTN, HTEm1, HTNm1, uarear};
   if (na > 0) {
-    for (int k = 0; k < 6; k++)
-      if (!idx[k]) return fail(EVP1D_ERR_INVALID_ARG, "neighbour vector %d is NULL", k);
-    for (int k = 0; k < 7; k++)
-      if (!geo[k]) return fail(EVP1D_ERR_INVALID_ARG, "geometry field %d is NULL", k);
+    if (!nonnull_all((const void *const *)idx, 6))
+      return fail(EVP1D_ERR_INVALID_ARG, "a neighbour vector is NULL");
+    if (!nonnull_all((const void *const *)geo, 7))
+      return fail(EVP1D_ERR_INVALID_ARG, "a geometry field is NULL");
   }
   // Host-side validation: every neighbour index must address a slot in
   // 1..navel, so no device gather can leave its buffer.
@@ -207,23 +224,25 @@ int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
     return fail(EVP1D_ERR_NO_DEVICE, "device %d is sm_%d%d; this build needs sm_100a",
                 device, prop.major, prop.minor);
 
+  // 0-based neighbour vectors and the tile plan (host)
+  std::vector<int32_t> nb0((size_t)na * 6);
+  const int32_t *nbp[6];
+  for (int k = 0; k < 6; k++) {
+    for (int w = 0; w < na; w++) nb0[(size_t)k * na + w] = idx[k][w] - 1;
+    nbp[k] = nb0.data() + (size_t)k * na;
+  }
+  evp::TilePlan plan;
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan);
+
   evp1d_t *h = new evp1d_handle();
-  h->device = device;
   h->p = to_params(*params);
-  int rc = evp::internal_alloc(h->device, na, navel, &h->s, &h->arena,
-                               &h->arena_bytes, &h->stream);
+  if (const char *e = getenv("EVP1D_PATH")) {
+    if (!strcmp(e, "fused")) h->path = kPathFused;
+  }
+  int rc = evp::problem_create(&h->d, device, plan, geo);
   if (rc != EVP1D_OK) {
+    evp::problem_destroy(&h->d);
     delete h;
-    return rc;
-  }
-  rc = evp::internal_upload_static(h->s, idx, geo, h->stream);
-  if (rc == EVP1D_OK) rc = select_device(h);
-  if (rc == EVP1D_OK) {
-    cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) rc = fail(EVP1D_ERR_CUDA, "init: %s", cudaGetErrorString(e));
-  }
-  if (rc != EVP1D_OK) {
-    evp1d_finalize(h);
     return rc;
   }
   *handle = h;
@@ -232,28 +251,32 @@ int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
 
 int evp1d_finalize(evp1d_t *h) {
   if (!h) return EVP1D_OK;
-  cudaSetDevice(h->device);
-  if (h->stream) cudaStreamSynchronize(h->stream);
-  drop_graph(h);
-  if (h->arena) cudaFree(h->arena);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  cudaSetDevice(h->d.device);
+  drop_graphs(h);
+  evp::problem_destroy(&h->d);
   delete h;
   return EVP1D_OK;
 }
 
 int evp1d_set_params(evp1d_t *h, const evp1d_params *params) {
   if (!h || !params) return fail(EVP1D_ERR_INVALID_ARG, "NULL argument");
+  CHECK(select_device(h));
+  const double old_rhow = h->p.rhow;
   h->p = to_params(*params);
-  drop_graph(h);
+  drop_graphs(h);
+  if (h->uploaded && h->p.rhow != old_rhow && h->d.nslots > 0) {
+    evp::launch_drag_factor(h->d.nslots, h->d.dyn[evp::kAiu], h->d.dyn[evp::kCw],
+                            h->p.rhow, h->d.dyn[evp::kKvrel], h->d.stream);
+    CUDA_TRY(cudaGetLastError());
+  }
   return EVP1D_OK;
 }
 
 int evp1d_upload(evp1d_t *h, const evp1d_fields *io) {
   if (!h || !io) return fail(EVP1D_ERR_INVALID_ARG, "NULL argument");
   CHECK(select_device(h));
-  CHECK(evp::internal_upload_fields(h->s, io, h->flags_host, h->stream));
+  CHECK(evp::problem_upload(&h->d, io, h->p.rhow));
   h->uploaded = true;
-  h->have_str = false;
   return EVP1D_OK;
 }
 
@@ -261,18 +284,26 @@ int evp1d_subcycles(evp1d_t *h, int ndte) {
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (ndte < 0) return fail(EVP1D_ERR_INVALID_ARG, "ndte = %d < 0", ndte);
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");
-  if (h->s.na == 0 || ndte == 0) return EVP1D_OK;
+  if (h->d.ntiles == 0 || ndte == 0) return EVP1D_OK;
   CHECK(select_device(h));
-  const int chunk = ndte < kGraphChunk ? ndte : kGraphChunk;
-  const int full = ndte / chunk, rest = ndte - full * chunk;
-  if (h->graph_n != chunk) CHECK(build_graph(h, chunk));
-  for (int k = 0; k < full; k++) {
-    CUDA_TRY(cudaGraphLaunch(h->graph, h->stream));
-    h->launches += 2LL * chunk;
+  cudaStream_t st = h->d.stream;
+  int body = ndte - 1;  // subcycles before the last one
+  while (body >= kGraphChunk) {
+    const int c = h->d.cur;
+    if (!h->graph[c]) CHECK(build_graph(h, c));
+    CUDA_TRY(cudaGraphLaunch(h->graph[c], st));
+    h->launches += kGraphChunk;
+    body -= kGraphChunk;
   }
-  if (rest) launch_subcycles_direct(h, rest);
+  for (; body > 0; body--) {
+    launch_sub(h, h->d.cur, false);
+    h->d.cur = 1 - h->d.cur;
+    h->launches++;
+  }
+  launch_sub(h, h->d.cur, true);
+  h->d.cur = 1 - h->d.cur;
+  h->launches++;
   CUDA_TRY(cudaGetLastError());
-  h->have_str = true;
   return EVP1D_OK;
 }
 
@@ -280,7 +311,8 @@ int evp1d_download(evp1d_t *h, const evp1d_fields *io) {
   if (!h || !io) return fail(EVP1D_ERR_INVALID_ARG, "NULL argument");
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "nothing uploaded");
   CHECK(select_device(h));
-  return evp::internal_download_fields(h->s, io, h->stream);
+  CHECK(check_device_error(h));
+  return evp::problem_download(&h->d, io);
 }
 
 int evp1d_run(evp1d_t *h, int ndte, const evp1d_fields *io) {
@@ -293,11 +325,12 @@ int evp1d_stress_only(evp1d_t *h, int n) {
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (n < 0) return fail(EVP1D_ERR_INVALID_ARG, "n = %d < 0", n);
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");
+  if (h->d.nslots == 0) return EVP1D_OK;
   CHECK(select_device(h));
-  for (int k = 0; k < n; k++) evp::launch_stress(h->s, h->p, h->stream);
-  h->launches += h->s.na > 0 ? n : 0;
+  const DevState s = evp::problem_inplace_view(h->d);
+  for (int k = 0; k < n; k++) evp::launch_stress(s, h->p, h->d.stream);
+  h->launches += n;
   CUDA_TRY(cudaGetLastError());
-  if (n > 0) h->have_str = true;
   return EVP1D_OK;
 }
 
@@ -305,9 +338,11 @@ int evp1d_stepu_only(evp1d_t *h, int n) {
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (n < 0) return fail(EVP1D_ERR_INVALID_ARG, "n = %d < 0", n);
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");
+  if (h->d.nslots == 0) return EVP1D_OK;
   CHECK(select_device(h));
-  for (int k = 0; k < n; k++) evp::launch_stepu(h->s, h->p, h->stream);
-  h->launches += h->s.na > 0 ? n : 0;
+  const DevState s = evp::problem_inplace_view(h->d);
+  for (int k = 0; k < n; k++) evp::launch_stepu(s, h->p, h->d.stream);
+  h->launches += n;
   CUDA_TRY(cudaGetLastError());
   return EVP1D_OK;
 }
@@ -315,11 +350,51 @@ int evp1d_stepu_only(evp1d_t *h, int n) {
 int evp1d_synchronize(evp1d_t *h) {
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   CHECK(select_device(h));
-  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->d.stream));
+  return check_device_error(h);
+}
+
+const char *evp1d_kernel_path(evp1d_t *h) {
+  if (!h) return "";
+  return h->path == kPathTma ? "fused-tile-tma" : "fused-tile";
+}
+
+int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
+                     const int32_t *se, const int32_t *nw, const int32_t *sw,
+                     const int32_t *sse, long long stats[8]) {
+  if (!stats || na < 0 || navel < na)
+    return fail(EVP1D_ERR_INVALID_ARG, "bad arguments");
+  const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
+  if (na > 0 && !nonnull_all((const void *const *)idx, 6))
+    return fail(EVP1D_ERR_INVALID_ARG, "a neighbour vector is NULL");
+  std::vector<int32_t> nb0((size_t)na * 6);
+  const int32_t *nbp[6];
+  for (int k = 0; k < 6; k++) {
+    for (int w = 0; w < na; w++) {
+      const int32_t v = idx[k][w];
+      if (v < 1 || v > navel) return fail(EVP1D_ERR_INDEX, "index out of range");
+      nb0[(size_t)k * na + w] = v - 1;
+    }
+    nbp[k] = nb0.data() + (size_t)k * na;
+  }
+  evp::TilePlan plan;
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan);
+  long long hmax = 0, tmax = 0;
+  for (int t = 0; t < plan.ntiles; t++) {
+    if (plan.halo_cnt[t] > hmax) hmax = plan.halo_cnt[t];
+    if (plan.tile_cnt[t] > tmax) tmax = plan.tile_cnt[t];
+  }
+  for (int k = 0; k < 8; k++) stats[k] = 0;
+  stats[0] = plan.ntiles;
+  stats[1] = plan.nslots;
+  stats[2] = (long long)plan.halo_idx.size();
+  stats[3] = plan.from_coords ? 1 : 0;
+  stats[4] = hmax;
+  stats[5] = tmax;
   return EVP1D_OK;
 }
 
-void *evp1d_stream(evp1d_t *h) { return h ? (void *)h->stream : nullptr; }
+void *evp1d_stream(evp1d_t *h) { return h ? (void *)h->d.stream : nullptr; }
 
 long long evp1d_launch_count(evp1d_t *h, int reset) {
   if (!h) return -1;

@@ -1,4 +1,4 @@
-// evp_internal.h -- library-internal helpers shared by the C-ABI translation
+// evp_internal.h -- library-internal state shared by the C-ABI translation
 // units (not part of the public ABI).
 #pragma once
 
@@ -9,28 +9,70 @@
 
 #include "evp1d.h"
 #include "evp_kernels.cuh"
+#include "evp_tiles.h"
 
 namespace evp {
 
 // Record `fmt` as this thread's last error message and return `code`.
 int error(int code, const char *fmt, ...);
 
-// One device arena for the whole problem; fills the pointers of `s` and
-// creates the handle's non-blocking stream.
-int internal_alloc(int device, int na, int navel, DevState *s, void **arena,
-                   size_t *bytes, cudaStream_t *stream);
+// Per-call input fields in the order they are staged and scattered.
+enum DynField {
+  kStrength, kCw, kAiu, kUocn, kVocn, kWaterx, kWatery, kForcex, kForcey,
+  kUmassdti, kFm, kTbu, kUinit, kVinit, kKvrel, kNumDyn
+};
+enum GeoField { kDxT, kDyT, kHTE, kHTN, kHTEm1, kHTNm1, kUarear, kNumGeo };
 
-// Neighbour vectors (1-based host -> 0-based device) and static geometry.
-int internal_upload_static(const DevState &s, const int32_t *const idx[6],
-                           const double *const geo[7], cudaStream_t st);
+// The 1D problem on one GPU in slot order (tiles of the TilePlan), with the
+// reference's halo slots appended after the nslots list slots for u, v, str.
+struct DeviceProblem {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int na = 0, navel = 0, nslots = 0, nhs = 0, nuv = 0, ntiles = 0;
+  bool from_coords = false;
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
+  // tile plan
+  int32_t *tile_off = nullptr, *tile_cnt = nullptr, *halo_off = nullptr;
+  int32_t *halo_cnt = nullptr, *halo_idx = nullptr;
+  int32_t *slot_of_point = nullptr, *point_of_slot = nullptr;
+  int32_t *nb[6] = {};  // ee ne se nw sw sse, slot space
+  uint32_t *lnb = nullptr;   // static packed stepu neighbours
+  uint32_t *meta = nullptr;  // lnb | skip flags << 30 (per call)
+  uint32_t *lcor = nullptr;  // packed stress corner velocity indices
+  uint32_t *halo_lcc = nullptr, *halo_lcor = nullptr;
+  int32_t *uvx_off = nullptr, *uvx_cnt = nullptr, *uvx_idx = nullptr;
+  int *err = nullptr;        // device error word of the bounded waits
+  int nctas = 0;             // persistent grid size (SM count)
+  uint8_t *flags = nullptr;
+  double *geo[kNumGeo] = {};
+  double *dyn[kNumDyn] = {};
+  double *stress[2][12] = {};
+  double *u[2] = {}, *v[2] = {};
+  double *strintx = nullptr, *strinty = nullptr, *Cb = nullptr;
+  double *str[8] = {};
+  double *stage = nullptr;  // reference-order staging, 32 x navel doubles
+  int cur = 0;              // buffer holding the current state
+};
 
-// Per-call fields host -> device; str is zeroed; uvel_init/vvel_init default
-// to uvel/vvel.  `flags_host` is a reusable host buffer.
-int internal_upload_fields(const DevState &s, const evp1d_fields *io,
-                           std::vector<uint8_t> &flags_host, cudaStream_t st);
+// Allocate and fill the static part from a tile plan and reference-order
+// geometry (host).  Creates the stream.
+int problem_create(DeviceProblem *d, int device, const TilePlan &plan,
+                   const double *const geo[kNumGeo]);
+void problem_destroy(DeviceProblem *d);
 
+// Per-call fields host -> device (through the staging area); str zeroed;
+// uvel_init/vvel_init default to the uploaded velocities; the drag factor
+// (aiu*rhow)*Cw is precomputed; cur = 0.
+int problem_upload(DeviceProblem *d, const evp1d_fields *io, double rhow);
 // Results device -> host; waits for the stream.
-int internal_download_fields(const DevState &s, const evp1d_fields *io,
-                             cudaStream_t st);
+int problem_download(DeviceProblem *d, const evp1d_fields *io);
+
+// Views for the kernels.
+DevState problem_inplace_view(const DeviceProblem &d);
+FusedArgs problem_fused_args(const DeviceProblem &d, int from);
+TmaArgs problem_tma_args(const DeviceProblem &d, int from);
+// Read and clear the device error word (0 if no bounded wait ran out).
+int problem_take_error(DeviceProblem *d, int *code);
 
 }  // namespace evp

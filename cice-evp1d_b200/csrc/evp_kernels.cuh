@@ -9,36 +9,115 @@
 
 namespace evp {
 
-// Skip flags packed per point: bit 0 = skipT, bit 1 = skipU.
+// Skip flags packed per slot: bit 0 = skipT, bit 1 = skipU.  Alignment
+// padding slots carry both bits.
 constexpr uint8_t kSkipT = 1;
 constexpr uint8_t kSkipU = 2;
 
-// Device-resident problem in the reference's 1D order (0-based indices).
-// uvel/vvel/str are navel long; the halo slots na..navel-1 of str stay 0.
+// Arrays of one in-place stress / stepu pass (the lindividual loops) over
+// `na` slots.  Indices address u, v and str, which have `navel` entries.
 struct DevState {
   int na = 0, navel = 0;
   const int32_t *ee = nullptr, *ne = nullptr, *se = nullptr;
   const int32_t *nw = nullptr, *sw = nullptr, *sse = nullptr;
   const uint8_t *flags = nullptr;
-  // static geometry [na]
   const double *dxT = nullptr, *dyT = nullptr, *HTE = nullptr, *HTN = nullptr;
   const double *HTEm1 = nullptr, *HTNm1 = nullptr, *uarear = nullptr;
-  // per-call inputs [na]
   const double *strength = nullptr, *Cw = nullptr, *aiu = nullptr;
   const double *uocn = nullptr, *vocn = nullptr, *waterx = nullptr;
   const double *watery = nullptr, *forcex = nullptr, *forcey = nullptr;
   const double *umassdti = nullptr, *fm = nullptr, *Tbu = nullptr;
   const double *uinit = nullptr, *vinit = nullptr;
-  // state
   double *stress[12] = {};
-  double *u = nullptr, *v = nullptr;  // [navel]
-  double *str[8] = {};                // [navel]
+  double *u = nullptr, *v = nullptr;
+  double *str[8] = {};
   double *strintx = nullptr, *strinty = nullptr, *Cb = nullptr;
 };
 
-// One stress pass over all list points (src/bench_v2b.F90:62-312).
+// One stress pass (src/bench_v2b.F90:62-312), in place.
 void launch_stress(const DevState &s, const Params &p, cudaStream_t st);
-// One stepu pass over all list points (src/bench_v2b.F90:444-549).
+// One stepu pass (src/bench_v2b.F90:444-549), in place.
 void launch_stepu(const DevState &s, const Params &p, cudaStream_t st);
+
+// One subcycle of the fused tile solver: stress on every tile's owned points
+// and forward halo, str in shared memory, stepu on the owned points.  Reads
+// the *_in state and writes the *_out state (ping-pong buffers).
+struct FusedArgs {
+  int ntiles = 0;
+  const int32_t *tile_off = nullptr, *tile_cnt = nullptr;
+  const int32_t *halo_off = nullptr, *halo_cnt = nullptr, *halo_idx = nullptr;
+  const uint8_t *flags = nullptr;
+  const int32_t *ee = nullptr, *ne = nullptr, *se = nullptr;
+  const uint32_t *lnb = nullptr;
+  const double *dxT = nullptr, *dyT = nullptr, *HTE = nullptr, *HTN = nullptr;
+  const double *HTEm1 = nullptr, *HTNm1 = nullptr, *strength = nullptr;
+  const double *kvrel = nullptr, *uocn = nullptr, *vocn = nullptr;
+  const double *waterx = nullptr, *watery = nullptr, *forcex = nullptr;
+  const double *forcey = nullptr, *umassdti = nullptr, *fm = nullptr;
+  const double *uarear = nullptr, *Tbu = nullptr, *uinit = nullptr;
+  const double *vinit = nullptr;
+  const double *u_in = nullptr, *v_in = nullptr;
+  double *u_out = nullptr, *v_out = nullptr;
+  const double *s_in[12] = {};
+  double *s_out[12] = {};
+  // written on the last subcycle of a call only
+  double *strintx = nullptr, *strinty = nullptr, *Cb = nullptr;
+  double *str_out[8] = {};
+};
+
+void launch_fused(const FusedArgs &a, const Params &p, bool last,
+                  cudaStream_t st);
+
+// The same subcycle as a persistent producer/consumer kernel fed by TMA bulk
+// copies (evp_kernels_tma.cu).  sf = 7 stress inputs (dxT, dyT, HTE, HTN,
+// HTEm1, HTNm1, strength) then the 12 input stresses; uf = 13 stepu inputs
+// (kvrel, uocn, vocn, waterx, watery, forcex, forcey, umassdti, fm, uarear,
+// Tbu, uinit, vinit).
+constexpr int kTmaStressFields = 19;
+constexpr int kTmaStepuFields = 13;
+struct TmaArgs {
+  int ntiles = 0;
+  const int32_t *tile_off = nullptr, *tile_cnt = nullptr;
+  const int32_t *halo_off = nullptr, *halo_cnt = nullptr, *halo_idx = nullptr;
+  const int32_t *uvx_off = nullptr, *uvx_cnt = nullptr, *uvx_idx = nullptr;
+  const uint32_t *meta = nullptr, *lcor = nullptr;
+  const uint32_t *halo_lcc = nullptr, *halo_lcor = nullptr;
+  const double *sf[kTmaStressFields] = {};
+  const double *uf[kTmaStepuFields] = {};
+  const double *u_in = nullptr, *v_in = nullptr;
+  double *u_out = nullptr, *v_out = nullptr;
+  double *s_out[12] = {};
+  double *strintx = nullptr, *strinty = nullptr, *Cb = nullptr;
+  double *str_out[8] = {};
+  int *err = nullptr;  // nonzero after a bounded wait ran out
+};
+
+// Allow the kernel's dynamic shared memory (call once per device).
+int tma_prepare(int device);
+void launch_tma(const TmaArgs &a, const Params &p, bool last, int nctas,
+                cudaStream_t st);
+
+// ---- layout conversion between the reference 1D order and slots ----------
+constexpr int kMaxBatch = 32;
+struct PermBatch {
+  int n = 0;
+  const double *src[kMaxBatch] = {};
+  double *dst[kMaxBatch] = {};
+  double *dst2[kMaxBatch] = {};  // optional second copy (ping-pong buffers)
+};
+// dst[f][s] = src[f][point_of_slot[s]] (0 for padding slots), s < nslots.
+void launch_scatter(const PermBatch &b, int nslots, const int32_t *point_of_slot,
+                    cudaStream_t st);
+// dst[f][p] = src[f][slot_of_point[p]], p < na.
+void launch_gather(const PermBatch &b, int na, const int32_t *slot_of_point,
+                   cudaStream_t st);
+// flags[s] from int32 skipT/skipU in reference order (padding: both bits);
+// meta[s] = lnb[s] | flags[s] << 30.
+void launch_flags(int nslots, const int32_t *point_of_slot,
+                  const int32_t *skipT, const int32_t *skipU, uint8_t *flags,
+                  const uint32_t *lnb, uint32_t *meta, cudaStream_t st);
+// kvrel[s] = (aiu[s]*rhow)*Cw[s].
+void launch_drag_factor(int nslots, const double *aiu, const double *Cw,
+                        double rhow, double *kvrel, cudaStream_t st);
 
 }  // namespace evp

@@ -1,0 +1,201 @@
+// evp_kernels_fused.cu -- one EVP subcycle per launch, one CTA per tile.
+//
+// Phase 1 (stress, src/bench_v2b.F90:126-311): every thread takes points of
+//   the tile's compute set -- its owned points followed by its forward halo
+//   (points reached through nw/sw/sse that another tile owns).  Velocities
+//   come from the previous subcycle's buffer; new stresses of owned points go
+//   to the other buffer; str1..str8 of every compute-set point go to shared
+//   memory (0 for skipT points, and a fixed zero slot stands for the
+//   reference's halo slots, whose str stays 0).
+// Phase 2 (stepu, src/bench_v2b.F90:506-547): one thread per owned point reads
+//   str of itself and of nw/sw/sse from shared memory and writes the new
+//   velocity to the other buffer.
+//
+// Recomputing the halo points' stress (owners compute the same values from
+// the same inputs with the same operations) keeps str on chip: per point and
+// subcycle the kernel moves the stress inputs and state, the stepu inputs and
+// the velocity, and never str1..str8.
+#include "evp_kernels.cuh"
+#include "evp_tiles.h"
+
+namespace evp {
+
+namespace {
+
+template <bool kLast>
+__global__ void __launch_bounds__(kTileOwned, 2)
+k_fused(FusedArgs a, Params p) {
+  __shared__ double s_str[8][kZeroSlot + 1];
+  const int t = blockIdx.x;
+  const int own = a.tile_cnt[t], base = a.tile_off[t];
+  const int nh = a.halo_cnt[t], hb = a.halo_off[t];
+  const int tid = threadIdx.x;
+  if (tid < 8) s_str[tid][kZeroSlot] = 0.0;
+
+  // ---------------- phase 1: stress on owned points + forward halo --------
+  for (int c = tid; c < own + nh; c += kTileOwned) {
+    const bool owned = c < own;
+    const int g = owned ? base + c : a.halo_idx[hb + (c - own)];
+    const int sidx = owned ? c : kTileOwned + (c - own);  // compute-set index
+    double out[8];
+    if (a.flags[g] & kSkipT) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) out[k] = 0.0;
+    } else {
+      const int iee = a.ee[g], ine = a.ne[g], ise = a.se[g];
+      Corners cr;
+      cr.ucc = a.u_in[g];
+      cr.vcc = a.v_in[g];
+      cr.uee = a.u_in[iee];
+      cr.vee = a.v_in[iee];
+      cr.une = a.u_in[ine];
+      cr.vne = a.v_in[ine];
+      cr.use = a.u_in[ise];
+      cr.vse = a.v_in[ise];
+      const Geom gm = make_geom(a.dxT[g], a.dyT[g], a.HTE[g], a.HTN[g],
+                                a.HTEm1[g], a.HTNm1[g], p.deltaminEVP);
+      const Strain sr = strain_rates(cr, gm, p.e_factor);
+      double st[12];
+#pragma unroll
+      for (int k = 0; k < 12; k++) st[k] = a.s_in[k][g];
+      stress_update(st, out, sr, a.strength[g], gm, p);
+      if (owned) {
+#pragma unroll
+        for (int k = 0; k < 12; k++) a.s_out[k][g] = st[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) s_str[k][sidx] = out[k];
+    if (kLast && owned) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) a.str_out[k][g] = out[k];
+    }
+  }
+  __syncthreads();
+
+  // ---------------- phase 2: stepu on owned points ------------------------
+  if (tid < own) {
+    const int g = base + tid;
+    if (!(a.flags[g] & kSkipU)) {
+      const uint32_t pk = a.lnb[g];
+      const int lnw = pk & kLnbMask;
+      const int lsw = (pk >> kLnbBits) & kLnbMask;
+      const int lsse = (pk >> (2 * kLnbBits)) & kLnbMask;
+      StepuIn in;
+      in.uold = a.u_in[g];
+      in.vold = a.v_in[g];
+      in.kvrel = a.kvrel[g];
+      in.uocn = a.uocn[g];
+      in.vocn = a.vocn[g];
+      in.waterx = a.waterx[g];
+      in.watery = a.watery[g];
+      in.forcex = a.forcex[g];
+      in.forcey = a.forcey[g];
+      in.umassdti = a.umassdti[g];
+      in.fm = a.fm[g];
+      in.uarear = a.uarear[g];
+      in.Tbu = a.Tbu[g];
+      in.uinit = a.uinit[g];
+      in.vinit = a.vinit[g];
+      in.s1 = s_str[0][tid];
+      in.s2nw = s_str[1][lnw];
+      in.s3sse = s_str[2][lsse];
+      in.s4sw = s_str[3][lsw];
+      in.s5 = s_str[4][tid];
+      in.s6sse = s_str[5][lsse];
+      in.s7nw = s_str[6][lnw];
+      in.s8sw = s_str[7][lsw];
+      const StepuOut o = stepu_point(in, p);
+      a.u_out[g] = o.u;
+      a.v_out[g] = o.v;
+      if (kLast) {
+        a.strintx[g] = o.strintx;
+        a.strinty[g] = o.strinty;
+        a.Cb[g] = o.Cb;
+      }
+    }
+  }
+}
+
+__global__ void k_scatter(PermBatch b, int nslots, const int32_t *pos) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots;
+       s += gridDim.x * blockDim.x) {
+    const int p = pos[s];
+    for (int f = 0; f < b.n; f++) {
+      const double v = p >= 0 ? b.src[f][p] : 0.0;
+      b.dst[f][s] = v;
+      if (b.dst2[f]) b.dst2[f][s] = v;
+    }
+  }
+}
+
+__global__ void k_gather(PermBatch b, int na, const int32_t *sop) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < na;
+       q += gridDim.x * blockDim.x) {
+    const int s = sop[q];
+    for (int f = 0; f < b.n; f++) b.dst[f][q] = b.src[f][s];
+  }
+}
+
+__global__ void k_flags(int nslots, const int32_t *pos, const int32_t *skipT,
+                        const int32_t *skipU, uint8_t *flags,
+                        const uint32_t *lnb, uint32_t *meta) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots;
+       s += gridDim.x * blockDim.x) {
+    const int p = pos[s];
+    const uint8_t f = p < 0 ? (uint8_t)(kSkipT | kSkipU)
+                            : (uint8_t)((skipT[p] ? kSkipT : 0) | (skipU[p] ? kSkipU : 0));
+    flags[s] = f;
+    meta[s] = lnb[s] | ((uint32_t)f << 30);
+  }
+}
+
+__global__ void k_drag(int n, const double *aiu, const double *Cw, double rhow,
+                       double *kv) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += gridDim.x * blockDim.x)
+    kv[s] = drag_factor(aiu[s], rhow, Cw[s]);
+}
+
+int blocks_for(int n) {
+  int b = (n + 255) / 256;
+  return b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b);
+}
+
+}  // namespace
+
+void launch_fused(const FusedArgs &a, const Params &p, bool last,
+                  cudaStream_t st) {
+  if (a.ntiles <= 0) return;
+  if (last)
+    k_fused<true><<<a.ntiles, kTileOwned, 0, st>>>(a, p);
+  else
+    k_fused<false><<<a.ntiles, kTileOwned, 0, st>>>(a, p);
+}
+
+void launch_scatter(const PermBatch &b, int nslots, const int32_t *pos,
+                    cudaStream_t st) {
+  if (nslots <= 0 || b.n <= 0) return;
+  k_scatter<<<blocks_for(nslots), 256, 0, st>>>(b, nslots, pos);
+}
+
+void launch_gather(const PermBatch &b, int na, const int32_t *sop,
+                   cudaStream_t st) {
+  if (na <= 0 || b.n <= 0) return;
+  k_gather<<<blocks_for(na), 256, 0, st>>>(b, na, sop);
+}
+
+void launch_flags(int nslots, const int32_t *pos, const int32_t *skipT,
+                  const int32_t *skipU, uint8_t *flags, const uint32_t *lnb,
+                  uint32_t *meta, cudaStream_t st) {
+  if (nslots <= 0) return;
+  k_flags<<<blocks_for(nslots), 256, 0, st>>>(nslots, pos, skipT, skipU, flags, lnb, meta);
+}
+
+void launch_drag_factor(int n, const double *aiu, const double *Cw,
+                        double rhow, double *kv, cudaStream_t st) {
+  if (n <= 0) return;
+  k_drag<<<blocks_for(n), 256, 0, st>>>(n, aiu, Cw, rhow, kv);
+}
+
+}  // namespace evp

@@ -53,8 +53,7 @@ k_stepu_ref(DevState s, Params p) {
     StepuIn in;
     in.uold = s.u[w];
     in.vold = s.v[w];
-    in.Cw = s.Cw[w];
-    in.aiX = s.aiu[w];
+    in.kvrel = drag_factor(s.aiu[w], p.rhow, s.Cw[w]);
     in.uocn = s.uocn[w];
     in.vocn = s.vocn[w];
     in.waterx = s.waterx[w];

@@ -210,10 +210,18 @@ __host__ __device__ __forceinline__ void stress_update(
            dxhy * csig12sw;
 }
 
-// Inputs of stepu at one U point (src/bench_v2b.F90:506-544).
+// Inputs of stepu at one U point (src/bench_v2b.F90:506-544).  kvrel is the
+// per-point factor aiX*rhow*Cw of the drag term, evaluated left to right
+// ((aiX*rhow)*Cw) as the reference does (:513); it does not change within a
+// call, so the fused path computes it once per call.
+__host__ __device__ __forceinline__ double drag_factor(double aiX, double rhow,
+                                                       double Cw) {
+  return aiX * rhow * Cw;
+}
+
 struct StepuIn {
   double uold, vold;
-  double Cw, aiX, uocn, vocn, waterx, watery, forcex, forcey;
+  double kvrel, uocn, vocn, waterx, watery, forcex, forcey;
   double umassdti, fm, uarear, Tbu, uinit, vinit;
   // str1(iw), str2(nw), str3(sse), str4(sw), str5(iw), str6(sse), str7(nw),
   // str8(sw)
@@ -229,7 +237,7 @@ __host__ __device__ __forceinline__ StepuOut stepu_point(const StepuIn &in,
   StepuOut o;
   const double uold = in.uold, vold = in.vold;
   const double du = in.uocn - uold, dv = in.vocn - vold;
-  const double vrel = in.aiX * p.rhow * in.Cw * sqrt(du * du + dv * dv);
+  const double vrel = in.kvrel * sqrt(du * du + dv * dv);
   const double taux = vrel * in.waterx;
   const double tauy = vrel * in.watery;
   o.Cb = in.Tbu / (sqrt(uold * uold + vold * vold) + p.u0);

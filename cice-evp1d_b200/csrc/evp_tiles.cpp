@@ -1,0 +1,308 @@
+// evp_tiles.cpp -- tile plan of the fused solver.
+//
+// Step 1: grid coordinates.  Either given (2D entry points) or rebuilt from
+//   the neighbour vectors by a breadth-first walk: ee = (i-1,j),
+//   ne = (i-1,j-1), se = (i,j-1), nw = (i+1,j), sw = (i+1,j+1),
+//   sse = (i,j+1) (integration/ice_dyn_evp1d.F90:766-772).  Each connected
+//   piece of the list gets its own origin.  A graph that contradicts itself
+//   (two coordinates for one point, or two points on one coordinate) has no
+//   grid layout, and the plan then tiles consecutive list points instead.
+// Step 2: tiles.  Points are grouped by (piece, j / kTileH, i / kTileW), tiles
+//   ordered row by row, points row by row inside a tile.
+// Step 3: forward halo.  A tile whose halo would exceed kTileHalo points is
+//   split in halves until it fits (possible only for irregular graphs).
+#include "evp_tiles.h"
+
+#include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <vector>
+
+namespace evp {
+
+namespace {
+
+const int kDI[6] = {-1, -1, 0, +1, +1, 0};  // ee ne se nw sw sse
+const int kDJ[6] = {0, -1, -1, 0, +1, +1};
+
+inline int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+bool reconstruct_coords(int na, const int32_t *const nb0[6],
+                        std::vector<int32_t> &ci, std::vector<int32_t> &cj,
+                        std::vector<int32_t> &comp) {
+  ci.assign((size_t)na, 0);
+  cj.assign((size_t)na, 0);
+  comp.assign((size_t)na, -1);
+  std::vector<int32_t> queue;
+  queue.reserve((size_t)na);
+  int ncomp = 0;
+  for (int p0 = 0; p0 < na; p0++) {
+    if (comp[p0] >= 0) continue;
+    comp[p0] = ncomp;
+    queue.clear();
+    queue.push_back(p0);
+    for (size_t h = 0; h < queue.size(); h++) {
+      const int q = queue[h];
+      for (int r = 0; r < 6; r++) {
+        const int n = nb0[r][q];
+        if (n < 0 || n >= na) continue;  // a halo slot, not a list point
+        const long long ei = (long long)ci[q] + kDI[r], ej = (long long)cj[q] + kDJ[r];
+        if (ei < INT_MIN / 2 || ei > INT_MAX / 2 || ej < INT_MIN / 2 || ej > INT_MAX / 2)
+          return false;
+        if (comp[n] < 0) {
+          comp[n] = ncomp;
+          ci[n] = (int32_t)ei;
+          cj[n] = (int32_t)ej;
+          queue.push_back(n);
+        } else if (comp[n] != ncomp || ci[n] != ei || cj[n] != ej) {
+          return false;
+        }
+      }
+    }
+    ncomp++;
+  }
+  // two points on one coordinate of one piece: no grid layout
+  std::vector<int32_t> order((size_t)na);
+  for (int p = 0; p < na; p++) order[p] = p;
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    if (comp[a] != comp[b]) return comp[a] < comp[b];
+    if (cj[a] != cj[b]) return cj[a] < cj[b];
+    return ci[a] < ci[b];
+  });
+  for (int k = 1; k < na; k++) {
+    const int a = order[k - 1], b = order[k];
+    if (comp[a] == comp[b] && ci[a] == ci[b] && cj[a] == cj[b]) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
+                     const int32_t *coords_i, const int32_t *coords_j,
+                     TilePlan *plan) {
+  TilePlan &P = *plan;
+  P = TilePlan();
+  P.na = na;
+  P.navel = navel;
+  P.nhalo_slots = navel - na;
+  if (na == 0) return;
+
+  // ---- step 1 + 2: candidate groups --------------------------------------
+  std::vector<std::vector<int32_t>> groups;
+  std::vector<int32_t> ci, cj, comp;
+  bool have = false;
+  if (coords_i && coords_j) {
+    ci.assign(coords_i, coords_i + na);
+    cj.assign(coords_j, coords_j + na);
+    comp.assign((size_t)na, 0);
+    have = true;
+  } else {
+    have = reconstruct_coords(na, nb0, ci, cj, comp);
+  }
+  P.from_coords = have;
+  if (have) {
+    // origin of each piece at its bounding-box corner, so that the tiles do
+    // not depend on where the walk started (i.e. on the list order)
+    int nc = 0;
+    for (int p = 0; p < na; p++) nc = comp[p] + 1 > nc ? comp[p] + 1 : nc;
+    std::vector<int32_t> mi((size_t)nc, INT_MAX), mj((size_t)nc, INT_MAX);
+    for (int p = 0; p < na; p++) {
+      mi[comp[p]] = ci[p] < mi[comp[p]] ? ci[p] : mi[comp[p]];
+      mj[comp[p]] = cj[p] < mj[comp[p]] ? cj[p] : mj[comp[p]];
+    }
+    for (int p = 0; p < na; p++) {
+      ci[p] -= mi[comp[p]];
+      cj[p] -= mj[comp[p]];
+    }
+    std::vector<int32_t> order((size_t)na);
+    for (int p = 0; p < na; p++) order[p] = p;
+    auto key = [&](int p, int &tj, int &ti) {
+      tj = floor_div(cj[p], kTileH);
+      ti = floor_div(ci[p], kTileW);
+    };
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+      int tja, tia, tjb, tib;
+      key(a, tja, tia);
+      key(b, tjb, tib);
+      if (comp[a] != comp[b]) return comp[a] < comp[b];
+      if (tja != tjb) return tja < tjb;
+      if (tia != tib) return tia < tib;
+      if (cj[a] != cj[b]) return cj[a] < cj[b];
+      return ci[a] < ci[b];
+    });
+    int k = 0;
+    while (k < na) {
+      int tj0, ti0;
+      key(order[k], tj0, ti0);
+      const int c0 = comp[order[k]];
+      std::vector<int32_t> g;
+      while (k < na) {
+        int tj, ti;
+        key(order[k], tj, ti);
+        if (comp[order[k]] != c0 || tj != tj0 || ti != ti0) break;
+        g.push_back(order[k]);
+        k++;
+      }
+      groups.push_back(std::move(g));
+    }
+  } else {
+    for (int k = 0; k < na; k += kTileOwned) {
+      std::vector<int32_t> g;
+      for (int p = k; p < na && p < k + kTileOwned; p++) g.push_back(p);
+      groups.push_back(std::move(g));
+    }
+  }
+
+  // ---- step 3: split groups whose halo or velocity set is too large ------
+  // halo H = list points outside the group reached through nw/sw/sse;
+  // extras X = ({H} + ee/ne/se of group and H) minus the group, where the
+  // reference's halo slots (>= na) count as points too.
+  std::vector<int32_t> mark((size_t)navel, -1), hmark((size_t)navel, -1),
+      xmark((size_t)navel, -1);
+  int stamp = 0;
+  std::vector<std::vector<int32_t>> tiles;
+  std::vector<std::vector<int32_t>> stack;
+  std::vector<int32_t> hl;
+  for (auto &g0 : groups) {
+    stack.push_back(std::move(g0));
+    while (!stack.empty()) {
+      std::vector<int32_t> g = std::move(stack.back());
+      stack.pop_back();
+      stamp++;
+      for (int p : g) mark[p] = stamp;
+      int nh = 0, nx = 0;
+      hl.clear();
+      for (int p : g)
+        for (int r = 3; r < 6; r++) {
+          const int n = nb0[r][p];
+          if (n < na && mark[n] != stamp && hmark[n] != stamp) {
+            hmark[n] = stamp;
+            hl.push_back(n);
+            nh++;
+          }
+        }
+      auto add_x = [&](int n) {
+        if (mark[n] != stamp && xmark[n] != stamp) {
+          xmark[n] = stamp;
+          nx++;
+        }
+      };
+      for (int q : hl) add_x(q);
+      for (int p : g)
+        for (int r = 0; r < 3; r++) add_x(nb0[r][p]);
+      for (int q : hl)
+        for (int r = 0; r < 3; r++) add_x(nb0[r][q]);
+      if ((int)g.size() <= kTileOwned && nh <= kTileHalo && nx <= kTileUvx) {
+        tiles.push_back(std::move(g));
+      } else {
+        const size_t half = g.size() / 2;
+        std::vector<int32_t> a(g.begin(), g.begin() + half), b(g.begin() + half, g.end());
+        stack.push_back(std::move(b));
+        stack.push_back(std::move(a));
+      }
+    }
+  }
+
+  // ---- slots ---------------------------------------------------------------
+  P.ntiles = (int)tiles.size();
+  P.tile_off.resize(P.ntiles);
+  P.tile_cnt.resize(P.ntiles);
+  P.slot_of_point.assign((size_t)na, -1);
+  std::vector<int32_t> tile_of((size_t)na, -1);
+  int off = 0;
+  for (int t = 0; t < P.ntiles; t++) {
+    P.tile_off[t] = off;
+    P.tile_cnt[t] = (int)tiles[t].size();
+    for (size_t k = 0; k < tiles[t].size(); k++) {
+      P.slot_of_point[tiles[t][k]] = off + (int)k;
+      tile_of[tiles[t][k]] = t;
+    }
+    off += ((int)tiles[t].size() + kSlotAlign - 1) / kSlotAlign * kSlotAlign;
+  }
+  P.nslots = off;
+  P.point_of_slot.assign((size_t)P.nslots, -1);
+  for (int p = 0; p < na; p++) P.point_of_slot[P.slot_of_point[p]] = p;
+
+  // ---- neighbour slots -------------------------------------------------------
+  auto to_slot = [&](int n) { return n < na ? P.slot_of_point[n] : P.nslots + (n - na); };
+  std::vector<int32_t> *arr[6] = {&P.ee, &P.ne, &P.se, &P.nw, &P.sw, &P.sse};
+  for (int r = 0; r < 6; r++) {
+    arr[r]->resize((size_t)P.nslots);
+    for (int s = 0; s < P.nslots; s++) {
+      const int p = P.point_of_slot[s];
+      (*arr[r])[s] = p < 0 ? s : to_slot(nb0[r][p]);
+    }
+  }
+
+  // ---- halo lists, velocity extras and packed local indices -----------------
+  const uint32_t zero3 = (uint32_t)kZeroSlot | ((uint32_t)kZeroSlot << kLnbBits) |
+                         ((uint32_t)kZeroSlot << (2 * kLnbBits));
+  P.lnb.assign((size_t)P.nslots, zero3);
+  P.lcor.assign((size_t)P.nslots, 0);
+  P.halo_off.resize(P.ntiles);
+  P.halo_cnt.resize(P.ntiles);
+  P.uvx_off.resize(P.ntiles);
+  P.uvx_cnt.resize(P.ntiles);
+  // hpos/htile: forward-halo position of a list point in the current tile;
+  // xpos/xtile: velocity-extra position of any u/v point (list or halo slot)
+  std::vector<int32_t> hpos((size_t)na, -1), htile((size_t)na, -1);
+  std::vector<int32_t> xpos((size_t)navel, -1), xtile((size_t)navel, -1);
+  for (int t = 0; t < P.ntiles; t++) {
+    P.halo_off[t] = (int)P.halo_idx.size();
+    P.uvx_off[t] = (int)P.uvx_idx.size();
+    int nh = 0, nx = 0;
+    const int own = P.tile_cnt[t];
+    std::vector<int32_t> &members = tiles[t];
+    // stepu's str neighbours and the forward halo
+    for (int k = 0; k < own; k++) {
+      const int p = members[k];
+      uint32_t packed = 0;
+      for (int r = 3; r < 6; r++) {
+        const int n = nb0[r][p];
+        uint32_t loc;
+        if (n >= na) {
+          loc = kZeroSlot;
+        } else if (tile_of[n] == t) {
+          loc = (uint32_t)(P.slot_of_point[n] - P.tile_off[t]);
+        } else {
+          if (htile[n] != t) {  // first time this tile reaches n
+            htile[n] = t;
+            hpos[n] = nh++;
+            P.halo_idx.push_back(P.slot_of_point[n]);
+          }
+          loc = (uint32_t)(kTileOwned + hpos[n]);
+        }
+        packed |= loc << ((r - 3) * kLnbBits);
+      }
+      P.lnb[P.slot_of_point[p]] = packed;
+    }
+    // velocity index of any u/v point n (list point or reference halo slot)
+    auto uv_local = [&](int n) -> uint32_t {
+      if (n < na && tile_of[n] == t) return (uint32_t)(P.slot_of_point[n] - P.tile_off[t]);
+      if (xtile[n] != t) {
+        xtile[n] = t;
+        xpos[n] = nx++;
+        P.uvx_idx.push_back(to_slot(n));
+      }
+      return (uint32_t)(kTileOwned + xpos[n]);
+    };
+    for (int k = 0; k < own; k++) {
+      const int p = members[k];
+      uint32_t packed = 0;
+      for (int r = 0; r < 3; r++) packed |= uv_local(nb0[r][p]) << (r * kLnbBits);
+      P.lcor[P.slot_of_point[p]] = packed;
+    }
+    for (int h = 0; h < nh; h++) {
+      const int q = P.point_of_slot[P.halo_idx[P.halo_off[t] + h]];
+      P.halo_lcc.push_back(uv_local(q));
+      uint32_t packed = 0;
+      for (int r = 0; r < 3; r++) packed |= uv_local(nb0[r][q]) << (r * kLnbBits);
+      P.halo_lcor.push_back(packed);
+    }
+    P.halo_cnt[t] = nh;
+    P.uvx_cnt[t] = nx;
+  }
+}
+
+}  // namespace evp

@@ -83,6 +83,18 @@ def build_index(mask: np.ndarray, nghost: int = 1):
     return n, nv, ti[:n], tj[:n], tij[:nv], {k: v[:n] for k, v in nb.items()}
 
 
+def plan_stats(na: int, navel: int, idx: dict) -> dict:
+    """Tile plan the solver builds for these 1-based neighbour vectors (host
+    only, no GPU)."""
+    L = _lib.load()
+    st = (C.c_longlong * 8)()
+    arrs = [_as_i32(idx[k], na, k) for k in ("ee", "ne", "se", "nw", "sw", "sse")]
+    check(L.evp1d_plan_stats(int(na), int(navel), *[a.ctypes.data_as(_I) for a in arrs], st),
+          "evp1d_plan_stats")
+    return dict(tiles=st[0], slots=st[1], halo=st[2], from_coords=bool(st[3]),
+                max_halo=st[4], max_tile=st[5])
+
+
 class FieldSet:
     """Host arrays of one dyn_evp1d_run call (evp1d_fields), kept alive while
     the ctypes struct points at them.  Arrays are updated in place by
@@ -208,7 +220,7 @@ class EVP1D:
     @property
     def path(self) -> str:
         """Name of the kernel path the library runs."""
-        return "two-kernel"
+        return self._L.evp1d_kernel_path(self.h).decode()
 
     @property
     def stream(self) -> int:

@@ -86,10 +86,13 @@ def load() -> C.CDLL:
     L.evp1d_last_error.restype = C.c_char_p
     L.evp1d_last_error.argtypes = []
     L.evp1d_version.restype = C.c_char_p
+    L.evp1d_kernel_path.argtypes = [H]
+    L.evp1d_kernel_path.restype = C.c_char_p
     L.evp1d_build_index.argtypes = ([C.c_int, C.c_int, C.c_int, _I, C.c_int,
                                      C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)] + [_I] * 9)
-    for name in ("evp1d_init", "evp1d_finalize", "evp1d_set_params",
+    L.evp1d_plan_stats.argtypes = [C.c_int, C.c_int] + [_I] * 6 + [C.POINTER(C.c_longlong)]
+    for name in ("evp1d_plan_stats", "evp1d_init", "evp1d_finalize", "evp1d_set_params",
                  "evp1d_run", "evp1d_upload", "evp1d_subcycles",
                  "evp1d_download", "evp1d_stress_only", "evp1d_stepu_only",
                  "evp1d_synchronize", "evp1d_build_index"):

@@ -11,6 +11,17 @@ once and neighbour gathers served from cache:
   12 stresses read + write (24), str1..8 written by stress and read by stepu
   (16), strintx/strinty/Cb written (3): 68 doubles = 544 B, plus 6 int32
   neighbour indices (24 B) and two 4-byte skip flags (8 B) = 576 B.
+* ``fused-tile`` -- one kernel per subcycle, str1..8 kept in shared memory,
+  ping-pong state: stress reads 7 inputs (dxT, dyT, HTE, HTN, HTEm1, HTNm1,
+  strength), the 12 stresses and u, v and writes the 12 stresses
+  (7 + 12 + 2 + 12 = 33 doubles); stepu reads 13 inputs (the drag factor
+  aiu*rhow*Cw, uocn, vocn, waterx, watery, forcex, forcey, umassdti, fm,
+  uarear, Tbu, uvel_init, vvel_init) and writes u, v (15 doubles); plus the
+  skip byte, 3 int32 stress neighbours and one packed int32 of local stepu
+  neighbours: 48 * 8 + 1 + 12 + 4 = 401 B.  The recomputed forward halo is
+  not algorithmic and shows up only in the measured traffic.
+* ``fused-tile-tma`` -- the same data flow with the tile's fields staged into
+  shared memory by TMA bulk copies: 401 B.
 """
 from __future__ import annotations
 
@@ -19,6 +30,8 @@ import os
 
 BYTES_PER_POINT_SUBCYCLE = {
     "two-kernel": 576,
+    "fused-tile": 401,
+    "fused-tile-tma": 401,
 }
 
 FALLBACK_HBM_GBS = 6650.0

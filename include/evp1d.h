@@ -133,8 +133,14 @@ int evp1d_download(evp1d_t *handle, const evp1d_fields *io);
 int evp1d_stress_only(evp1d_t *handle, int n);
 int evp1d_stepu_only(evp1d_t *handle, int n);
 
-/* Wait for the handle's stream. */
+/* Wait for the handle's stream.  Returns EVP1D_ERR_TIMEOUT if a bounded
+ * device-side wait of the solver ran out since the last check. */
 int evp1d_synchronize(evp1d_t *handle);
+
+/* Name of the subcycle kernel the handle runs: "fused-tile-tma" (default,
+ * TMA-fed persistent kernel) or "fused-tile" (plain loads; selected by the
+ * environment variable EVP1D_PATH=fused at evp1d_init). */
+const char *evp1d_kernel_path(evp1d_t *handle);
 
 /* The handle's CUDA stream (a cudaStream_t), for event timing by callers. */
 void *evp1d_stream(evp1d_t *handle);
@@ -163,6 +169,18 @@ int evp1d_build_index(int nx, int ny, int nghost, const int32_t *mask,
                       int32_t *indxti, int32_t *indxtj, int32_t *indxtij,
                       int32_t *ee, int32_t *ne, int32_t *se, int32_t *nw,
                       int32_t *sw, int32_t *sse);
+
+/* ----------------------------------------------------------------------------
+ * Host-only diagnostics of the tile plan the solver would build for a 1D
+ * problem (same arguments as evp1d_init, 1-based neighbours; no GPU needed).
+ * stats[0] tiles, [1] device slots (list points + alignment padding),
+ * [2] forward-halo points summed over tiles, [3] 1 if the tiles follow grid
+ * coordinates rebuilt from the neighbour vectors (0: consecutive list points),
+ * [4] largest halo of one tile, [5] largest tile.
+ * -------------------------------------------------------------------------- */
+int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
+                     const int32_t *se, const int32_t *nw, const int32_t *sw,
+                     const int32_t *sse, long long stats[8]);
 
 #ifdef __cplusplus
 }

@@ -75,3 +75,51 @@ def first_mismatch(a: np.ndarray, b: np.ndarray) -> str:
     i = ne[0]
     rel = np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))
     return f"{ne.size} differ; first at {i}: {a[i]!r} vs {b[i]!r}; max rel {rel:.3e}"
+
+
+def shuffle_problem(pr: synth.Problem1D, seed: int) -> synth.Problem1D:
+    """Relabel the list points in a random order (halo slots keep their
+    numbers).  Every point computes the same values, so results are the
+    original ones permuted; the solver must rebuild the grid from the graph."""
+    rng = np.random.default_rng(seed)
+    na = pr.na
+    perm = rng.permutation(na)          # new position of old point p
+    inv = np.empty(na, np.int64)
+    inv[perm] = np.arange(na)           # old point at new position q
+    q = pr.copy()
+    def remap(v):
+        v = v.astype(np.int64)
+        out = v.copy()
+        m = v <= na
+        out[m] = perm[v[m] - 1] + 1
+        return out.astype(np.int32)
+    q.idx = {k: remap(v)[inv] for k, v in pr.idx.items()}
+    q.skipT, q.skipU = pr.skipT[inv], pr.skipU[inv]
+    q.f = {k: v[inv] for k, v in pr.f.items()}
+    q.stress = pr.stress[:, inv]
+    q.uvel = np.concatenate([pr.uvel[:na][inv], pr.uvel[na:]])
+    q.vvel = np.concatenate([pr.vvel[:na][inv], pr.vvel[na:]])
+    q.strintx, q.strinty, q.Cb = pr.strintx[inv], pr.strinty[inv], pr.Cb[inv]
+    q.indxti = q.indxtj = None
+    return q
+
+
+def random_graph_problem(na: int, nhalo: int, seed: int) -> synth.Problem1D:
+    """A 1D problem whose neighbour vectors are random slots: no grid layout
+    exists, which exercises the consecutive-point tiling and halo splitting."""
+    rng = np.random.default_rng(seed)
+    navel = na + nhalo
+    base = synth.make_problem("cfg1", nx=60, ny=50, seed=seed, ndte=5)
+    reps = -(-na // base.na)
+    f = {k: np.tile(v, reps)[:na].copy() for k, v in base.f.items()}
+    idx = {k: rng.integers(1, navel + 1, na).astype(np.int32)
+           for k in ("ee", "ne", "se", "nw", "sw", "sse")}
+    skipT = (rng.random(na) < 0.1).astype(np.int32)
+    skipU = (rng.random(na) < 0.1).astype(np.int32)
+    uvel = np.concatenate([rng.normal(0, 0.05, na), np.zeros(nhalo)])
+    vvel = np.concatenate([rng.normal(0, 0.05, na), np.zeros(nhalo)])
+    f["uvel_init"], f["vvel_init"] = uvel[:na].copy(), vvel[:na].copy()
+    return synth.Problem1D(na=na, navel=navel, ndte=5, idx=idx, skipT=skipT,
+                           skipU=skipU, f=f, stress=np.zeros((12, na)),
+                           uvel=uvel, vvel=vvel, strintx=np.zeros(na),
+                           strinty=np.zeros(na), Cb=np.zeros(na))

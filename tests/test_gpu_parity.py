@@ -72,6 +72,9 @@ def test_two_calls_carry_state(oracle_mod):
     pr2.uvel[:] = st.uvel[: pr.navel]
     pr2.vvel[:] = st.vvel[: pr.navel]
     pr2.strintx[:], pr2.strinty[:], pr2.Cb[:] = st.strintx, st.strinty, st.Cb
+    # the second call's uvel_init defaults to its starting velocity
+    pr2.f["uvel_init"] = st.uvel[: pr.na].copy()
+    pr2.f["vvel_init"] = st.vvel[: pr.na].copy()
     assert_same(fs, oracle_run(oracle_mod, pr2, 10), pr2)
 
 
@@ -192,3 +195,42 @@ def test_launch_count_is_native():
         s.launch_count(reset=True)
         s.run(7, fs)
         assert s.launch_count() > 0
+
+
+def test_shuffled_list_order(oracle_mod):
+    """A list in random order: the solver rebuilds the grid tiles from the
+    neighbour graph; results stay bitwise equal."""
+    pr = helpers.shuffle_problem(synth.make_problem("cfg1", nx=90, ny=70, ndte=9), 7)
+    assert_same(gpu_run(pr, 9), oracle_run(oracle_mod, pr, 9), pr)
+
+
+@pytest.mark.parametrize("na,nhalo,seed", [(5000, 300, 0), (777, 5, 1)])
+def test_irregular_graph(oracle_mod, na, nhalo, seed):
+    """Random neighbour slots (no grid): consecutive-point tiles whose halo
+    is split to fit; results stay bitwise equal."""
+    pr = helpers.random_graph_problem(na, nhalo, seed)
+    assert_same(gpu_run(pr, 5), oracle_run(oracle_mod, pr, 5), pr)
+
+
+@pytest.mark.parametrize("ndte", [1, 2, 49, 50, 51, 101])
+def test_graph_chunk_boundaries(oracle_mod, ndte):
+    """Subcycle counts around the captured-graph chunk (50) and both
+    ping-pong parities."""
+    pr = synth.make_problem("cfg1", nx=40, ny=30, ndte=ndte)
+    assert_same(gpu_run(pr, ndte), oracle_run(oracle_mod, pr, ndte), pr)
+
+
+@pytest.mark.parametrize("path", ["fused", "tma"])
+def test_kernel_paths(oracle_mod, monkeypatch, path):
+    """Both subcycle kernels (plain loads and TMA-fed) are bitwise equal to
+    the oracle; EVP1D_PATH selects the kernel at evp1d_init."""
+    if path == "fused":
+        monkeypatch.setenv("EVP1D_PATH", "fused")
+    else:
+        monkeypatch.delenv("EVP1D_PATH", raising=False)
+    pr = synth.make_problem("cfg1", nx=150, ny=110, ndte=11)
+    fs = evp1d.FieldSet.from_problem(pr, want_str=True)
+    with evp1d.EVP1D.from_problem(pr, ndte=11) as s:
+        assert s.path == ("fused-tile" if path == "fused" else "fused-tile-tma")
+        s.run(11, fs)
+    assert_same(fs, oracle_run(oracle_mod, pr, 11), pr)

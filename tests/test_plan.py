@@ -1,0 +1,48 @@
+"""CPU tests of the fused solver's tile plan (evp1d_plan_stats): grid tiles
+are rebuilt from the neighbour graph whatever the list order, irregular
+graphs fall back to consecutive points, and no tile exceeds its limits."""
+import numpy as np
+import pytest
+
+import evp1d
+from evp1d import synth
+import helpers
+
+
+def stats(pr):
+    return evp1d.plan_stats(pr.na, pr.navel, pr.idx)
+
+
+def test_cfg1_plan_uses_grid_tiles():
+    s = stats(synth.make_problem("cfg1"))
+    assert s["from_coords"] and s["max_halo"] <= 16 + 16 + 1 and s["max_tile"] <= 256
+    assert s["halo"] < 0.2 * s["slots"]
+
+
+def test_shuffled_list_still_finds_grid():
+    pr = synth.make_problem("cfg1", nx=90, ny=70)
+    a = stats(pr)
+    b = stats(helpers.shuffle_problem(pr, 4))
+    assert b["from_coords"]
+    assert (a["tiles"], a["halo"]) == (b["tiles"], b["halo"])
+
+
+@pytest.mark.parametrize("na,nhalo,seed", [(5000, 300, 0), (777, 5, 1), (1, 1, 2)])
+def test_random_graph_falls_back(na, nhalo, seed):
+    pr = helpers.random_graph_problem(na, nhalo, seed)
+    s = stats(pr)
+    assert s["max_halo"] <= 256 and s["max_tile"] <= 256
+    if na > 10:
+        assert not s["from_coords"]
+
+
+def test_standalone_plan():
+    s = stats(helpers.standalone_problem())
+    # 21 x 21 square in 16 x 16 tiles: at most 4 tiles
+    assert s["from_coords"] and s["tiles"] <= 4 and s["slots"] >= 441
+
+
+def test_empty_plan():
+    z = np.zeros(0, np.int32)
+    s = evp1d.plan_stats(0, 0, {k: z for k in ("ee", "ne", "se", "nw", "sw", "sse")})
+    assert s["tiles"] == 0 and s["slots"] == 0
