@@ -293,12 +293,14 @@ def main():
         e1.record(stream)
         e1.synchronize()
         e2e_times.append(e0.elapsed_time(e1) / 1000.0)
-    t_e2e = statistics.median(e2e_times)
-    if pg:
-        t = torch.tensor([t_e2e], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e_value = pr.n_active * ndte * world / t_e2e
+    e2e_value = None
+    if e2e_times:
+        t_e2e = statistics.median(e2e_times)
+        if pg:
+            t = torch.tensor([t_e2e], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e_value = pr.n_active * ndte * world / t_e2e
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

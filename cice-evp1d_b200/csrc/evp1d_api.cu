@@ -80,6 +80,8 @@ struct evp1d_handle {
   DeviceProblem d;
   Params p{};
   int path = kPathTma;
+  int prefetch = 0;  // L2 prefetch distance of the TMA kernel (tiles)
+  long long *trace = nullptr;  // device timing trace (EVP1D_TRACE, debug)
   bool uploaded = false;
   long long launches = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // by starting buffer
@@ -101,10 +103,14 @@ void drop_graphs(evp1d_t *h) {
 
 // One subcycle from buffer `from` into the other one.
 void launch_sub(evp1d_t *h, int from, bool last) {
-  if (h->path == kPathTma)
-    evp::launch_tma(evp::problem_tma_args(h->d, from), h->p, last, h->d.nctas, h->d.stream);
-  else
+  if (h->path == kPathTma) {
+    evp::TmaArgs a = evp::problem_tma_args(h->d, from);
+    a.prefetch = h->prefetch;
+    a.trace = h->trace;
+    evp::launch_tma(a, h->p, last, h->d.nctas, h->d.stream);
+  } else {
     evp::launch_fused(evp::problem_fused_args(h->d, from), h->p, last, h->d.stream);
+  }
 }
 
 // A bounded device-side wait that ran out leaves a code in the error word.
@@ -239,6 +245,16 @@ int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
   if (const char *e = getenv("EVP1D_PATH")) {
     if (!strcmp(e, "fused")) h->path = kPathFused;
   }
+  if (getenv("EVP1D_TRACE")) {
+    if (cudaMalloc(&h->trace, sizeof(long long) * 8 * evp::kTraceTiles) != cudaSuccess)
+      h->trace = nullptr;
+    else
+      cudaMemset(h->trace, 0, sizeof(long long) * 8 * evp::kTraceTiles);
+  }
+  if (const char *e = getenv("EVP1D_PREFETCH")) {
+    const int v = atoi(e);
+    h->prefetch = v < 0 ? 0 : (v > 8 ? 8 : v);
+  }
   int rc = evp::problem_create(&h->d, device, plan, geo);
   if (rc != EVP1D_OK) {
     evp::problem_destroy(&h->d);
@@ -254,6 +270,7 @@ int evp1d_finalize(evp1d_t *h) {
   cudaSetDevice(h->d.device);
   drop_graphs(h);
   evp::problem_destroy(&h->d);
+  if (h->trace) cudaFree(h->trace);
   delete h;
   return EVP1D_OK;
 }
@@ -352,6 +369,16 @@ int evp1d_synchronize(evp1d_t *h) {
   CHECK(select_device(h));
   CUDA_TRY(cudaStreamSynchronize(h->d.stream));
   return check_device_error(h);
+}
+
+int evp1d_debug_trace(evp1d_t *h, long long *out, int n) {
+  if (!h || !out || n < 0) return fail(EVP1D_ERR_INVALID_ARG, "bad arguments");
+  if (!h->trace) return fail(EVP1D_ERR_STATE, "tracing is off (set EVP1D_TRACE)");
+  if (n > 8 * evp::kTraceTiles) n = 8 * evp::kTraceTiles;
+  CHECK(select_device(h));
+  CUDA_TRY(cudaStreamSynchronize(h->d.stream));
+  CUDA_TRY(cudaMemcpy(out, h->trace, sizeof(long long) * (size_t)n, cudaMemcpyDeviceToHost));
+  return EVP1D_OK;
 }
 
 const char *evp1d_kernel_path(evp1d_t *h) {

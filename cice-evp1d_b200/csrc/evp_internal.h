@@ -42,6 +42,8 @@ struct DeviceProblem {
   uint32_t *lcor = nullptr;  // packed stress corner velocity indices
   uint32_t *halo_lcc = nullptr, *halo_lcor = nullptr;
   int32_t *uvx_off = nullptr, *uvx_cnt = nullptr, *uvx_idx = nullptr;
+  int32_t *tile_meta = nullptr;  // 8 int32 per tile (see TmaArgs)
+  int32_t *tile_rec = nullptr;   // kRecInts int32 per tile (producer records)
   int *err = nullptr;        // device error word of the bounded waits
   int nctas = 0;             // persistent grid size (SM count)
   uint8_t *flags = nullptr;

@@ -82,6 +82,10 @@ struct TmaArgs {
   const int32_t *uvx_off = nullptr, *uvx_cnt = nullptr, *uvx_idx = nullptr;
   const uint32_t *meta = nullptr, *lcor = nullptr;
   const uint32_t *halo_lcc = nullptr, *halo_lcor = nullptr;
+  // per tile 8 int32: off, cnt, uvx_off, uvx_cnt, halo_off, halo_cnt, 0, 0
+  const int32_t *tile_meta = nullptr;
+  // per tile one producer record of kRecInts int32 (evp_tiles.h)
+  const int32_t *tile_rec = nullptr;
   const double *sf[kTmaStressFields] = {};
   const double *uf[kTmaStepuFields] = {};
   const double *u_in = nullptr, *v_in = nullptr;
@@ -90,7 +94,13 @@ struct TmaArgs {
   double *strintx = nullptr, *strinty = nullptr, *Cb = nullptr;
   double *str_out[8] = {};
   int *err = nullptr;  // nonzero after a bounded wait ran out
+  int prefetch = 0;    // tiles prefetched into L2 ahead of the shared ring
+  // optional timing trace of block 0 (debug): per tile 8 %globaltimer stamps
+  // [0] producer issued, [1] A got the stage, [2] A corners done, [3] A str
+  // done, [4] B got the stage, [5] B done; kTraceTiles tiles at most
+  long long *trace = nullptr;
 };
+constexpr int kTraceTiles = 256;
 
 // Allow the kernel's dynamic shared memory (call once per device).
 int tma_prepare(int device);

@@ -23,7 +23,10 @@ namespace evp {
 namespace {
 
 template <bool kLast>
-__global__ void __launch_bounds__(kTileOwned, 2)
+#ifndef EVP_FUSED_MIN_BLOCKS
+#define EVP_FUSED_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(kTileOwned, EVP_FUSED_MIN_BLOCKS)
 k_fused(FusedArgs a, Params p) {
   __shared__ double s_str[8][kZeroSlot + 1];
   const int t = blockIdx.x;

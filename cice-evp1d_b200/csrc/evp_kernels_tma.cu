@@ -10,9 +10,12 @@
 //   - the forward-halo points (recomputed stress) and the extra velocity
 //     points of the stencil are gathered with 4/8-byte cp.async, whose
 //     completion arrives on the same mbarrier (cp.async.mbarrier.arrive).
+// The producer's own inputs -- the tile's slot range and gather lists -- are
+// one 1.3 KB record per tile that a bulk copy brings kRecRing tiles ahead,
+// so the producer never waits on a global load.
 // Ten consumer warps (one thread per compute-set point: 256 owned + 64 halo)
-// compute stress from shared memory into the shared str table, then stepu
-// for the owned points, writing the new stresses and velocities to the other
+// compute stress from shared memory into the shared str table, then stepu for
+// the owned points, writing the new stresses and velocities to the other
 // ping-pong buffer.  While they compute tile k the producer loads tile k+1.
 //
 // Every mbarrier wait is bounded by %globaltimer (kWaitNs): on expiry the
@@ -29,6 +32,7 @@ namespace evp {
 namespace {
 
 constexpr int kStages = 2;
+constexpr int kRecRing = 4;                         // producer records in flight
 constexpr int kConsumers = kTileOwned + kTileHalo;  // 320 = 10 warps
 constexpr int kThreads = kConsumers + 32;           // + 1 producer warp
 constexpr int kUV = kTileOwned + kTileUvx;
@@ -45,17 +49,21 @@ struct Stage {
   uint32_t hmeta[kTileHalo];
   uint32_t hlcc[kTileHalo];
   uint32_t hlcor[kTileHalo];
+  int hdr[4];  // tile offset, owned count, halo count (written by the producer)
 };
 
 struct Smem {
   Stage st[kStages];
-  double str[8][kZeroSlot + 1];
+  double str[8][kZeroSlot + 2];
+  int32_t rec[kRecRing][kRecInts];
   unsigned long long full[kStages];
   unsigned long long empty[kStages];
+  unsigned long long rec_full[kRecRing];
   int abort_flag;
 };
 
 static_assert(sizeof(Stage) % 16 == 0, "stage must keep 16-byte alignment");
+static_assert((kRecInts * 4) % 16 == 0, "records are bulk-copied");
 
 // ---------------- PTX helpers -------------------------------------------------
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -123,6 +131,11 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// Bulk prefetch of global memory into L2 (no shared memory, no completion).
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src)
                : "memory");
@@ -140,8 +153,18 @@ __device__ __forceinline__ void cp_async_arrive(unsigned long long *bar) {
                : "memory");
 }
 
+// Order this thread's generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) accesses to the same memory.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void consumer_sync() {
   asm volatile("bar.sync 1, %0;" ::"r"(kConsumers) : "memory");
+}
+
+__device__ __forceinline__ void trace_stamp(const TmaArgs &a, int it, int slot) {
+  if (a.trace && blockIdx.x == 0 && it < kTraceTiles) a.trace[it * 8 + slot] = (long long)global_ns();
 }
 
 // ---------------- the kernel ---------------------------------------------------
@@ -156,6 +179,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       mbar_init(&S.full[s], 1 + 32);  // expect_tx arrival + 32 cp.async lanes
       mbar_init(&S.empty[s], 1);      // one consumer arrival per use
     }
+    for (int r = 0; r < kRecRing; r++) mbar_init(&S.rec_full[r], 1);
     S.abort_flag = 0;
     mbar_fence_init();
   }
@@ -165,49 +189,96 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   if (tid >= kConsumers) {
     // ======================= producer warp ==============================
     const int lane = tid - kConsumers;
+    const int T0 = blockIdx.x, dT = gridDim.x;
+    constexpr uint32_t kRecBytes = kRecInts * 4u;
+    if (lane == 0) {
+      for (int r = 0; r < kRecRing; r++) {
+        const int t = T0 + r * dT;
+        if (t >= a.ntiles) break;
+        mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
+        bulk_g2s(S.rec[r], a.tile_rec + (size_t)t * kRecInts, kRecBytes, &S.rec_full[r]);
+      }
+    }
     int issued = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    for (int t = T0; t < a.ntiles; t += dT) {
+      const int r = issued % kRecRing;
+      int w = 1;
+      if (lane == 0) w = mbar_wait(&S.rec_full[r], (uint32_t)(issued / kRecRing) & 1, a.err, 6);
       const int s = issued % kStages;
       const uint32_t use = (uint32_t)(issued / kStages);
-      if (issued >= kStages) {
-        int w = 1;
-        if (lane == 0) w = mbar_wait(&S.empty[s], (use - 1) & 1, a.err, 2) ? 1 : 0;
-        w = __shfl_sync(0xffffffffu, w, 0);
-        if (!w) {
-          ok = false;
-          break;
-        }
+      if (w && issued >= kStages && lane == 0)
+        w = mbar_wait(&S.empty[s], (use - 1) & 1, a.err, 2) ? 1 : 0;
+      w = __shfl_sync(0xffffffffu, w, 0);
+      if (!w) {
+        ok = false;
+        break;
       }
+      const int32_t *rec = S.rec[r];
+      const int off = rec[0], cnt = rec[1], nx = rec[2], nh = rec[3];
       Stage &st = S.st[s];
-      const int off = a.tile_off[t], cnt = a.tile_cnt[t];
-      const uint32_t n4 = (uint32_t)((cnt + 3) & ~3);
+      for (int h = lane; h < nh; h += 32) {
+        st.hlcor[h] = (uint32_t)rec[kRecHLcor + h];
+        st.hlcc[h] = (uint32_t)rec[kRecHLcc + h];
+      }
       if (lane == 0) {
-        const uint32_t b8 = n4 * 8u, b4 = n4 * 4u;
+        st.hdr[0] = off;
+        st.hdr[1] = cnt;
+        st.hdr[2] = nh;
+      }
+      __syncwarp();
+      const uint32_t n4 = (uint32_t)((cnt + 3) & ~3);
+      const uint32_t b8 = n4 * 8u, b4 = n4 * 4u;
+      // release: the header and halo indices are visible to consumers once
+      // the phase completes
+      if (lane == 0)
         mbar_arrive_expect_tx(&S.full[s],
                               (kTmaStressFields + kTmaStepuFields + 2) * b8 + 2 * b4);
-        for (int f = 0; f < kTmaStressFields; f++) bulk_g2s(st.sf[f], a.sf[f] + off, b8, &S.full[s]);
-        for (int f = 0; f < kTmaStepuFields; f++) bulk_g2s(st.uf[f], a.uf[f] + off, b8, &S.full[s]);
-        bulk_g2s(st.u, a.u_in + off, b8, &S.full[s]);
-        bulk_g2s(st.v, a.v_in + off, b8, &S.full[s]);
-        bulk_g2s(st.meta, a.meta + off, b4, &S.full[s]);
-        bulk_g2s(st.lcor, a.lcor + off, b4, &S.full[s]);
+      __syncwarp();
+      for (int k = lane; k < kTmaStressFields + kTmaStepuFields + 4; k += 32) {
+        if (k < kTmaStressFields)
+          bulk_g2s(st.sf[k], a.sf[k] + off, b8, &S.full[s]);
+        else if (k < kTmaStressFields + kTmaStepuFields)
+          bulk_g2s(st.uf[k - kTmaStressFields], a.uf[k - kTmaStressFields] + off, b8, &S.full[s]);
+        else if (k == kTmaStressFields + kTmaStepuFields)
+          bulk_g2s(st.u, a.u_in + off, b8, &S.full[s]);
+        else if (k == kTmaStressFields + kTmaStepuFields + 1)
+          bulk_g2s(st.v, a.v_in + off, b8, &S.full[s]);
+        else if (k == kTmaStressFields + kTmaStepuFields + 2)
+          bulk_g2s(st.meta, a.meta + off, b4, &S.full[s]);
+        else
+          bulk_g2s(st.lcor, a.lcor + off, b4, &S.full[s]);
       }
-      const int xo = a.uvx_off[t], nx = a.uvx_cnt[t];
       for (int x = lane; x < nx; x += 32) {
-        const int g = a.uvx_idx[xo + x];
+        const int g = rec[kRecUvx + x];
         cp_async8(&st.u[kTileOwned + x], a.u_in + g);
         cp_async8(&st.v[kTileOwned + x], a.v_in + g);
       }
-      const int ho = a.halo_off[t], nh = a.halo_cnt[t];
       for (int h = lane; h < nh; h += 32) {
-        const int g = a.halo_idx[ho + h];
+        const int g = rec[kRecHalo + h];
         for (int f = 0; f < kTmaStressFields; f++) cp_async8(&st.hf[f][h], a.sf[f] + g);
         cp_async4(&st.hmeta[h], a.meta + g);
-        cp_async4(&st.hlcc[h], a.halo_lcc + ho + h);
-        cp_async4(&st.hlcor[h], a.halo_lcor + ho + h);
       }
       cp_async_arrive(&S.full[s]);
+      if (lane == 0) trace_stamp(a, issued, 0);
+      // record slot r has been read: refill it kRecRing tiles ahead
+      fence_proxy_async();
+      __syncwarp();
+      const int tr = t + kRecRing * dT;
+      if (lane == 0 && tr < a.ntiles) {
+        mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
+        bulk_g2s(S.rec[r], a.tile_rec + (size_t)tr * kRecInts, kRecBytes, &S.rec_full[r]);
+      }
+      if (a.prefetch > 0) {
+        const int tp = t + a.prefetch * dT;
+        if (tp < a.ntiles && lane < 2) {
+          // the owned slot range of every staged field of a later tile
+          const int po = a.tile_meta[8 * tp], pc = a.tile_meta[8 * tp + 1];
+          const uint32_t pn = (uint32_t)((pc + 3) & ~3);
+          for (int f = lane; f < kTmaStressFields; f += 2) bulk_prefetch_l2(a.sf[f] + po, pn * 8u);
+          for (int f = lane; f < kTmaStepuFields; f += 2) bulk_prefetch_l2(a.uf[f] + po, pn * 8u);
+        }
+      }
       issued++;
     }
     if (!ok) {
@@ -217,8 +288,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
         if (k < 0) continue;
         if (lane == 0) mbar_wait(&S.full[k % kStages], (uint32_t)(k / kStages) & 1, a.err, 3);
       }
-      __syncwarp();
     }
+    // records issued ahead and never consumed must land before exit too
+    if (lane == 0) {
+      for (int k = issued; k < issued + kRecRing; k++) {
+        const int t = T0 + k * dT;
+        if (t >= a.ntiles) break;
+        mbar_wait(&S.rec_full[k % kRecRing], (uint32_t)(k / kRecRing) & 1, a.err, 7);
+      }
+    }
+    __syncwarp();
     return;
   }
 
@@ -231,8 +310,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     if (!mbar_wait(&S.full[s], use & 1, a.err, 1)) S.abort_flag = 1;
     consumer_sync();
     if (S.abort_flag) break;
+    if (tid == 0) trace_stamp(a, it, 1);
     const Stage &st = S.st[s];
-    const int off = a.tile_off[t], cnt = a.tile_cnt[t], nh = a.halo_cnt[t];
+    const int off = st.hdr[0], cnt = st.hdr[1], nh = st.hdr[2];
 
     // ---------------- phase 1: stress ------------------------------------
     const bool own = c < kTileOwned;
@@ -279,6 +359,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       }
     }
     consumer_sync();
+    if (tid == 0) trace_stamp(a, it, 2);
 
     // ---------------- phase 2: stepu on owned points ------------------------
     if (c < cnt) {
@@ -321,7 +402,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       }
     }
     consumer_sync();  // stage s and the str table are free again
-    if (c == 0) mbar_arrive(&S.empty[s]);
+    if (tid == 0) {
+      trace_stamp(a, it, 5);
+      mbar_arrive(&S.empty[s]);
+    }
   }
 }
 

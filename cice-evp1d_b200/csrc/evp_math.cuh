@@ -103,15 +103,83 @@ __host__ __device__ __forceinline__ Strain strain_rates(const Corners &c,
 }
 
 // visc_replpress (src/bench_v2b.F90:415-437).
+//
+// Exact shortcuts (each result bit-identical to the literal formula):
+//  - capping == 1: tmpcalc = 1*x + 0*q with x = strength/max(Delta,DminArea)
+//    and q = strength/(Delta+DminArea).  1*x is x; 0*q is a zero carrying
+//    q's sign, and q has x's sign, so x + 0*q is x -- provided q is finite
+//    and Delta is not NaN.  Both hold when strength is finite, DminArea > 0
+//    and |strength| < 1e300*DminArea (then |q| <= |strength|/DminArea), so
+//    the second division is skipped under exactly those conditions.
+//  - Ktens == 0: (1+Ktens)*t and (1-Ktens)*t are 1*t, which is t.
 __host__ __device__ __forceinline__ void visc_replpress(
     double strength, double DminArea, double Delta, const Params &p,
     double &zetax2, double &etax2, double &rep_prs) {
-  const double tmpcalc = p.capping * (strength / fmax_ref(Delta, DminArea)) +
-                         (kC1 - p.capping) * (strength / (Delta + DminArea));
-  zetax2 = (kC1 + p.Ktens) * tmpcalc;
-  rep_prs = (kC1 - p.Ktens) * tmpcalc * Delta;
+  double tmpcalc;
+  const bool capped = p.capping == kC1 && Delta == Delta && DminArea > 0.0 &&
+                      fabs(strength) < 1e300 * DminArea;
+  if (capped)
+    tmpcalc = strength / fmax_ref(Delta, DminArea);
+  else
+    tmpcalc = p.capping * (strength / fmax_ref(Delta, DminArea)) +
+              (kC1 - p.capping) * (strength / (Delta + DminArea));
+  if (p.Ktens == 0.0) {
+    zetax2 = tmpcalc;
+    rep_prs = tmpcalc * Delta;
+  } else {
+    zetax2 = (kC1 + p.Ktens) * tmpcalc;
+    rep_prs = (kC1 - p.Ktens) * tmpcalc * Delta;
+  }
   etax2 = p.epp2i * zetax2;
 }
+
+// One corner's stress relaxation (src/bench_v2b.F90:170-212): viscosities
+// from Delta, then stressp_k, stressm_k, stress12_k updated in place.
+__host__ __device__ __forceinline__ void corner_update(
+    double &sp, double &sm, double &s12, double div, double ten, double shr,
+    double Delta, double strength, double DminTarea, const Params &p) {
+  double z, e, r;
+  visc_replpress(strength, DminTarea, Delta, p, z, e, r);
+  const double arlx1i = p.arlx1i, denom1 = p.denom1, revp = p.revp;
+  sp = (sp * (kC1 - arlx1i * revp) + arlx1i * (z * div - r)) * denom1;
+  sm = (sm * (kC1 - arlx1i * revp) + arlx1i * e * ten) * denom1;
+  s12 = (s12 * (kC1 - arlx1i * revp) + arlx1i * kP5 * e * shr) * denom1;
+}
+
+// Strain rates and Delta of corner k (0 ne, 1 nw, 2 sw, 3 se) in one
+// branch-free form, so that the four corners of a point can run on four lanes
+// of a warp.  With P1 = (cc, ee, ne, se)[k], P2 = (ee, cc, se, ne)[k] and
+// P4 = (se, ne, ee, cc)[k], the reference's twelve expressions
+// (src/bench_v2b.F90:363-395) are
+//   div = ((A1*u[P1] + B2*u[P2]) + A3*v[P1]) + B4*v[P4]
+//   ten = ((-(C1*u[P1]) + B2*u[P2]) + C3*v[P1]) + (-B4)*v[P4]
+//   shr = ((-(C1*v[P1]) + B2*v[P2]) + (-C3)*u[P1]) + B4*u[P4]
+// with A1 = (cyp,cym,cym,cyp), C1 = (cym,cyp,cyp,cym), A3 = (cxp,cxp,cxm,cxm),
+// C3 = (cxm,cxm,cxp,cxp), B2 = (-dyT,dyT,dyT,-dyT), B4 = (-dxT,-dxT,dxT,dxT).
+// Every product and sum is the reference's own: a - b is a + (-b) and
+// (-a)*b is -(a*b) exactly in IEEE arithmetic.
+__host__ __device__ __forceinline__ void corner_strain(
+    int k, double u1, double v1, double u2, double v2, double u4, double v4,
+    const Geom &g, double e_factor, double &div, double &ten, double &shr,
+    double &Delta) {
+  const bool a = (k == 0) | (k == 3);
+  const bool b = k < 2;
+  const double A1 = a ? g.cyp : g.cym;
+  const double C1 = a ? g.cym : g.cyp;
+  const double A3 = b ? g.cxp : g.cxm;
+  const double C3 = b ? g.cxm : g.cxp;
+  const double B2 = a ? -g.dyT : g.dyT;
+  const double B4 = b ? -g.dxT : g.dxT;
+  div = A1 * u1 + B2 * u2 + A3 * v1 + B4 * v4;
+  ten = -(C1 * u1) + B2 * u2 + C3 * v1 + (-B4) * v4;
+  shr = -(C1 * v1) + B2 * v2 + (-C3) * u1 + B4 * u4;
+  Delta = sqrt(div * div + e_factor * (ten * ten + shr * shr));
+}
+
+// The 8 str combinations of the updated stresses (src/bench_v2b.F90:217-310).
+__host__ __device__ __forceinline__ void str_combine(const double (&s)[12],
+                                                     double (&out)[8],
+                                                     const Geom &g);
 
 // The 12 corner stress relaxations and the 8 str combinations
 // (src/bench_v2b.F90:186-310).  s[0..11] = stressp_1..4, stressm_1..4,
@@ -119,25 +187,18 @@ __host__ __device__ __forceinline__ void visc_replpress(
 __host__ __device__ __forceinline__ void stress_update(
     double (&s)[12], double (&out)[8], const Strain &sr, double strength,
     const Geom &g, const Params &p) {
-  double z[4], e[4], r[4];
-#pragma unroll
-  for (int k = 0; k < 4; k++)
-    visc_replpress(strength, g.DminTarea, sr.Delta[k], p, z[k], e[k], r[k]);
-  const double arlx1i = p.arlx1i, denom1 = p.denom1, revp = p.revp;
   // corner k of the reference (1=ne, 2=nw, 3=sw, 4=se) uses ne/nw/sw/se
   // strain: index map 1->0 (ne), 2->1 (nw), 3->2 (sw), 4->3 (se).
 #pragma unroll
   for (int k = 0; k < 4; k++)
-    s[k] = (s[k] * (kC1 - arlx1i * revp) +
-            arlx1i * (z[k] * sr.div[k] - r[k])) * denom1;
-#pragma unroll
-  for (int k = 0; k < 4; k++)
-    s[4 + k] = (s[4 + k] * (kC1 - arlx1i * revp) +
-                arlx1i * e[k] * sr.ten[k]) * denom1;
-#pragma unroll
-  for (int k = 0; k < 4; k++)
-    s[8 + k] = (s[8 + k] * (kC1 - arlx1i * revp) +
-                arlx1i * kP5 * e[k] * sr.shr[k]) * denom1;
+    corner_update(s[k], s[4 + k], s[8 + k], sr.div[k], sr.ten[k], sr.shr[k],
+                  sr.Delta[k], strength, g.DminTarea, p);
+  str_combine(s, out, g);
+}
+
+__host__ __device__ __forceinline__ void str_combine(const double (&s)[12],
+                                                     double (&out)[8],
+                                                     const Geom &g) {
 
   const double ssigpn = s[0] + s[1];
   const double ssigps = s[2] + s[3];
@@ -232,6 +293,16 @@ struct StepuOut {
   double u, v, strintx, strinty, Cb;
 };
 
+// stepu at one point (src/bench_v2b.F90:509-544).
+//
+// Exact shortcuts (each result bit-identical to the literal formula):
+//  - Tbu == +0, u0 > 0 and u, v not NaN: the denominator sqrt(u^2+v^2)+u0
+//    is positive or +Inf, so Cb = +0 without the square root and division;
+//  - cosw == 1: vrel*cosw is vrel;
+//  - sinw == 0: sign(1,fm)*vrel*0 is a signed zero, and fm + (that zero) is
+//    fm unless fm is -0 and the zero is +0, i.e. unless fm == -0 and
+//    vrel < 0; a NaN vrel takes the literal route; an infinite vrel makes u
+//    and v NaN on both routes, and strintx, strinty and Cb do not use ccb.
 __host__ __device__ __forceinline__ StepuOut stepu_point(const StepuIn &in,
                                                          const Params &p) {
   StepuOut o;
@@ -240,9 +311,13 @@ __host__ __device__ __forceinline__ StepuOut stepu_point(const StepuIn &in,
   const double vrel = in.kvrel * sqrt(du * du + dv * dv);
   const double taux = vrel * in.waterx;
   const double tauy = vrel * in.watery;
-  o.Cb = in.Tbu / (sqrt(uold * uold + vold * vold) + p.u0);
-  const double cca = (p.brlx + p.revp) * in.umassdti + vrel * p.cosw + o.Cb;
-  const double ccb = in.fm + copysign(kC1, in.fm) * vrel * p.sinw;
+  const bool tbu_zero = in.Tbu == 0.0 && copysign(kC1, in.Tbu) > 0.0 && p.u0 > 0.0 &&
+                        uold == uold && vold == vold;
+  o.Cb = tbu_zero ? 0.0 : in.Tbu / (sqrt(uold * uold + vold * vold) + p.u0);
+  const double cca = (p.brlx + p.revp) * in.umassdti + (p.cosw == kC1 ? vrel : vrel * p.cosw) + o.Cb;
+  const double ccb = p.sinw == 0.0 && (in.fm != 0.0 || vrel >= 0.0)
+                         ? in.fm
+                         : in.fm + copysign(kC1, in.fm) * vrel * p.sinw;
   const double ab2 = cca * cca + ccb * ccb;
   o.strintx = in.uarear * (in.s1 + in.s2nw + in.s3sse + in.s4sw);
   o.strinty = in.uarear * (in.s5 + in.s6sse + in.s7nw + in.s8sw);

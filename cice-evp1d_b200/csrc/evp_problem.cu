@@ -60,6 +60,8 @@ void layout(DeviceProblem *d, Carve &c, size_t nhalo_total, size_t nuvx_total) {
   c.take(&d->uvx_off, T);
   c.take(&d->uvx_cnt, T);
   c.take(&d->uvx_idx, nuvx_total);
+  c.take(&d->tile_meta, 8 * T);
+  c.take(&d->tile_rec, (size_t)kRecInts * T);
   c.take(&d->tile_off, T);
   c.take(&d->tile_cnt, T);
   c.take(&d->halo_off, T);
@@ -135,6 +137,33 @@ int problem_create(DeviceProblem *d, int device, const TilePlan &plan,
   TRY(h2d(d->uvx_off, plan.uvx_off.data(), T, st));
   TRY(h2d(d->uvx_cnt, plan.uvx_cnt.data(), T, st));
   TRY(h2d(d->uvx_idx, plan.uvx_idx.data(), plan.uvx_idx.size() * sizeof(int32_t), st));
+  std::vector<int32_t> tm((size_t)8 * d->ntiles, 0);
+  for (int t = 0; t < d->ntiles; t++) {
+    int32_t *q = tm.data() + (size_t)8 * t;
+    q[0] = plan.tile_off[t];
+    q[1] = plan.tile_cnt[t];
+    q[2] = plan.uvx_off[t];
+    q[3] = plan.uvx_cnt[t];
+    q[4] = plan.halo_off[t];
+    q[5] = plan.halo_cnt[t];
+  }
+  TRY(h2d(d->tile_meta, tm.data(), tm.size() * sizeof(int32_t), st));
+  std::vector<int32_t> rec((size_t)kRecInts * d->ntiles, 0);
+  for (int t = 0; t < d->ntiles; t++) {
+    int32_t *q = rec.data() + (size_t)kRecInts * t;
+    const int nx = plan.uvx_cnt[t], nh = plan.halo_cnt[t];
+    q[0] = plan.tile_off[t];
+    q[1] = plan.tile_cnt[t];
+    q[2] = nx;
+    q[3] = nh;
+    for (int x = 0; x < nx; x++) q[kRecUvx + x] = plan.uvx_idx[plan.uvx_off[t] + x];
+    for (int h = 0; h < nh; h++) {
+      q[kRecHalo + h] = plan.halo_idx[plan.halo_off[t] + h];
+      q[kRecHLcor + h] = (int32_t)plan.halo_lcor[plan.halo_off[t] + h];
+      q[kRecHLcc + h] = (int32_t)plan.halo_lcc[plan.halo_off[t] + h];
+    }
+  }
+  TRY(h2d(d->tile_rec, rec.data(), rec.size() * sizeof(int32_t), st));
   // geometry: reference order -> staging -> slots
   PermBatch b;
   for (int k = 0; k < kNumGeo; k++) {
@@ -409,6 +438,8 @@ TmaArgs problem_tma_args(const DeviceProblem &d, int from) {
   a.lcor = d.lcor;
   a.halo_lcc = d.halo_lcc;
   a.halo_lcor = d.halo_lcor;
+  a.tile_meta = d.tile_meta;
+  a.tile_rec = d.tile_rec;
   const int geo_order[6] = {kDxT, kDyT, kHTE, kHTN, kHTEm1, kHTNm1};
   for (int k = 0; k < 6; k++) a.sf[k] = d.geo[geo_order[k]];
   a.sf[6] = d.dyn[kStrength];

@@ -22,7 +22,17 @@ constexpr int kTileH = 16;        // tile height in j
 //  compute set (str):  owned c -> c, forward halo h -> kTileOwned + h,
 //                      kZeroSlot -> a slot holding str = 0;
 //  velocities (u, v):  owned c -> c, extra x -> kTileOwned + x.
-constexpr int kZeroSlot = kTileOwned + kTileHalo;
+constexpr int kTileCompute = kTileOwned + kTileHalo;
+constexpr int kZeroSlot = kTileCompute;
+// Per-tile producer record (int32): [0] slot offset, [1] owned count,
+// [2] extra velocity count, [3] halo count, [4..7] unused, then the extra
+// velocity slots, the halo slots, the halo points' packed corner indices and
+// their own velocity indices.
+constexpr int kRecUvx = 8;
+constexpr int kRecHalo = kRecUvx + kTileUvx;
+constexpr int kRecHLcor = kRecHalo + kTileHalo;
+constexpr int kRecHLcc = kRecHLcor + kTileHalo;
+constexpr int kRecInts = kRecHLcc + kTileHalo;
 constexpr int kSlotAlign = 4;     // tile starts are multiples of 4 slots (32 B)
 constexpr int kLnbBits = 10;      // bits per packed local index
 constexpr uint32_t kLnbMask = (1u << kLnbBits) - 1;

@@ -86,6 +86,8 @@ def load() -> C.CDLL:
     L.evp1d_last_error.restype = C.c_char_p
     L.evp1d_last_error.argtypes = []
     L.evp1d_version.restype = C.c_char_p
+    L.evp1d_debug_trace.argtypes = [H, C.POINTER(C.c_longlong), C.c_int]
+    L.evp1d_debug_trace.restype = C.c_int
     L.evp1d_kernel_path.argtypes = [H]
     L.evp1d_kernel_path.restype = C.c_char_p
     L.evp1d_build_index.argtypes = ([C.c_int, C.c_int, C.c_int, _I, C.c_int,

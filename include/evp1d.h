@@ -137,6 +137,12 @@ int evp1d_stepu_only(evp1d_t *handle, int n);
  * device-side wait of the solver ran out since the last check. */
 int evp1d_synchronize(evp1d_t *handle);
 
+/* Debug: timing trace of the TMA kernel's block 0 in the last launch
+ * (recorded only when EVP1D_TRACE is set at evp1d_init).  Up to 256 tiles x 8
+ * %globaltimer stamps (ns): producer issued, group A got the stage, corners
+ * done, str done, group B got the stage, stepu done, 2 unused. */
+int evp1d_debug_trace(evp1d_t *handle, long long *out, int n);
+
 /* Name of the subcycle kernel the handle runs: "fused-tile-tma" (default,
  * TMA-fed persistent kernel) or "fused-tile" (plain loads; selected by the
  * environment variable EVP1D_PATH=fused at evp1d_init). */

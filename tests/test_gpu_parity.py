@@ -234,3 +234,42 @@ def test_kernel_paths(oracle_mod, monkeypatch, path):
         assert s.path == ("fused-tile" if path == "fused" else "fused-tile-tma")
         s.run(11, fs)
     assert_same(fs, oracle_run(oracle_mod, pr, 11), pr)
+
+
+def assert_same_nan_aware(fs, st, pr):
+    """Bitwise equality, except that NaN must meet NaN (GPU and x86 produce
+    different NaN payloads)."""
+    na = pr.na
+    for name, a, b in (("stress", fs.stress, st.stress), ("uvel", fs.uvel[:na], st.uvel[:na]),
+                       ("vvel", fs.vvel[:na], st.vvel[:na]), ("strintx", fs.strintx, st.strintx),
+                       ("strinty", fs.strinty, st.strinty), ("Cb", fs.Cb, st.Cb)):
+        a = np.asarray(a).reshape(-1)
+        b = np.asarray(b).reshape(-1)
+        assert np.array_equal(np.isnan(a), np.isnan(b)), f"{name}: NaN pattern differs"
+        m = ~np.isnan(b)
+        assert np.array_equal(a[m].view(np.int64), b[m].view(np.int64)), \
+            f"{name}: {helpers.first_mismatch(a[m], b[m])}"
+
+
+@pytest.mark.parametrize("u0", [5e-5, 0.0])
+def test_shortcut_edges(oracle_mod, u0):
+    """Inputs at the edges of the solver's exact shortcuts: signed zeros in
+    Tbu and fm, negative drag factors, zero strength, zero cell area (no
+    Delta floor), resting ice with u0 = 0 (0/0 in Cb)."""
+    pr = synth.make_problem("cfg1", nx=60, ny=44, seed=13, ndte=7)
+    rng = np.random.default_rng(9)
+    n = pr.na
+    pick = lambda f: rng.random(n) < f
+    pr.f["Tbu"] = np.where(pick(0.3), -0.0, np.where(pick(0.3), 0.0, rng.uniform(0, 3, n)))
+    pr.f["fm"] = np.where(pick(0.2), -0.0, np.where(pick(0.2), 0.0, pr.f["fm"]))
+    pr.f["aiu"] = np.where(pick(0.1), -pr.f["aiu"], pr.f["aiu"])
+    pr.f["strength"] = np.where(pick(0.1), 0.0, np.where(pick(0.05), -0.0, pr.f["strength"]))
+    pr.f["dxT"] = np.where(pick(0.03), 0.0, pr.f["dxT"])
+    rest = pick(0.1)
+    pr.uvel[:n] = np.where(rest, 0.0, pr.uvel[:n])
+    pr.vvel[:n] = np.where(rest, 0.0, pr.vvel[:n])
+    pr.f["uvel_init"], pr.f["vvel_init"] = pr.uvel[:n].copy(), pr.vvel[:n].copy()
+    p = evp1d.set_evp_parameters(7)
+    p.u0 = u0
+    fs = gpu_run(pr, 7, params=p)
+    assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 7, params=p), pr)
