@@ -85,6 +85,13 @@ struct evp1d_handle {
   bool uploaded = false;
   long long launches = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // by starting buffer
+  // ensemble (batched) handles: caller arrays are member-major concatenations
+  // with each member's halo slots after its list points; uv_pos maps the
+  // combined slot order (all list points, then all halo slots) to them.
+  int nmembers = 1;
+  std::vector<int64_t> uv_pos;
+  std::vector<double> uv_tmp;  // scratch for u, v (and str) in combined order
+  std::string tuned;           // last autotuner choice
 };
 
 namespace {
@@ -186,37 +193,11 @@ void evp1d_set_evp_parameters(evp1d_params *p, int ndte) {
   p->deltaminEVP = 10e-9;
 }
 
-int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
-               const int32_t *ne, const int32_t *se, const int32_t *nw,
-               const int32_t *sw, const int32_t *sse, const double *dxT,
-               const double *dyT, const double *HTE, const double *HTN,
-               const double *HTEm1, const double *HTNm1, const double *uarear,
-               const evp1d_params *params, int device) {
-  g_err.clear();
-  if (!handle) return fail(EVP1D_ERR_INVALID_ARG, "handle is NULL");
-  *handle = nullptr;
-  if (na < 0 || navel < na)
-    return fail(EVP1D_ERR_INVALID_ARG, "need 0 <= na <= navel (na=%d navel=%d)",
-                na, navel);
-  if (!params) return fail(EVP1D_ERR_INVALID_ARG, "params is NULL");
-  const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
-  const double *geo[7] = {dxT, dyT, HTE, HTN, HTEm1, HTNm1, uarear};
-  if (na > 0) {
-    if (!nonnull_all((const void *const *)idx, 6))
-      return fail(EVP1D_ERR_INVALID_ARG, "a neighbour vector is NULL");
-    if (!nonnull_all((const void *const *)geo, 7))
-      return fail(EVP1D_ERR_INVALID_ARG, "a geometry field is NULL");
-  }
-  // Host-side validation: every neighbour index must address a slot in
-  // 1..navel, so no device gather can leave its buffer.
-  static const char *nbname[6] = {"ee", "ne", "se", "nw", "sw", "sse"};
-  for (int k = 0; k < 6; k++)
-    for (int w = 0; w < na; w++) {
-      const int32_t v = idx[k][w];
-      if (v < 1 || v > navel)
-        return fail(EVP1D_ERR_INDEX, "%s(%d) = %d outside 1..%d", nbname[k],
-                    w + 1, (int)v, navel);
-    }
+}  // extern "C"
+
+namespace {
+
+int check_device(int device) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
     cudaGetLastError();
@@ -229,8 +210,13 @@ int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
   if (prop.major != 10)
     return fail(EVP1D_ERR_NO_DEVICE, "device %d is sm_%d%d; this build needs sm_100a",
                 device, prop.major, prop.minor);
+  return EVP1D_OK;
+}
 
-  // 0-based neighbour vectors and the tile plan (host)
+// Validated 1-based neighbour vectors -> tile plan -> device problem.
+int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6],
+                const double *const geo[7], const evp1d_params *params, int device) {
+  CHECK(check_device(device));
   std::vector<int32_t> nb0((size_t)na * 6);
   const int32_t *nbp[6];
   for (int k = 0; k < 6; k++) {
@@ -258,10 +244,151 @@ int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
   int rc = evp::problem_create(&h->d, device, plan, geo);
   if (rc != EVP1D_OK) {
     evp::problem_destroy(&h->d);
+    if (h->trace) cudaFree(h->trace);
     delete h;
     return rc;
   }
   *handle = h;
+  return EVP1D_OK;
+}
+
+int validate_neighbours(int na, int navel, const int32_t *const idx[6], int member) {
+  static const char *nbname[6] = {"ee", "ne", "se", "nw", "sw", "sse"};
+  for (int k = 0; k < 6; k++)
+    for (int w = 0; w < na; w++) {
+      const int32_t v = idx[k][w];
+      if (v < 1 || v > navel) {
+        if (member < 0)
+          return fail(EVP1D_ERR_INDEX, "%s(%d) = %d outside 1..%d", nbname[k], w + 1, (int)v,
+                      navel);
+        return fail(EVP1D_ERR_INDEX, "member %d: %s(%d) = %d outside 1..%d", member,
+                    nbname[k], w + 1, (int)v, navel);
+      }
+    }
+  return EVP1D_OK;
+}
+
+// Fields of a batched handle with u, v (and str) reordered into the combined
+// slot order; `io` is the caller's member-major layout.
+evp1d_fields combined_view(evp1d_t *h, const evp1d_fields *io, bool fill) {
+  evp1d_fields c = *io;
+  const size_t nv = h->uv_pos.size();
+  int nstr = 0;
+  for (int k = 0; k < 8; k++) nstr += io->str[k] ? 1 : 0;
+  h->uv_tmp.resize(nv * (size_t)(2 + nstr));
+  double *u = h->uv_tmp.data(), *v = u + nv;
+  if (fill) {
+    for (size_t k = 0; k < nv; k++) {
+      u[k] = io->uvel[h->uv_pos[k]];
+      v[k] = io->vvel[h->uv_pos[k]];
+    }
+  }
+  c.uvel = u;
+  c.vvel = v;
+  int q = 0;
+  for (int k = 0; k < 8; k++) c.str[k] = io->str[k] ? u + (size_t)(2 + q++) * nv : nullptr;
+  return c;
+}
+
+void scatter_combined(evp1d_t *h, const evp1d_fields *io, int na_total) {
+  const size_t nv = h->uv_pos.size();
+  const double *u = h->uv_tmp.data(), *v = u + nv;
+  for (int k = 0; k < na_total; k++) {  // list slots are updated; halo slots are not
+    io->uvel[h->uv_pos[k]] = u[k];
+    io->vvel[h->uv_pos[k]] = v[k];
+  }
+  int q = 0;
+  for (int k = 0; k < 8; k++)
+    if (io->str[k]) {
+      const double *s = u + (size_t)(2 + q++) * nv;
+      for (size_t w = 0; w < nv; w++) io->str[k][h->uv_pos[w]] = s[w];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
+               const int32_t *ne, const int32_t *se, const int32_t *nw,
+               const int32_t *sw, const int32_t *sse, const double *dxT,
+               const double *dyT, const double *HTE, const double *HTN,
+               const double *HTEm1, const double *HTNm1, const double *uarear,
+               const evp1d_params *params, int device) {
+  g_err.clear();
+  if (!handle) return fail(EVP1D_ERR_INVALID_ARG, "handle is NULL");
+  *handle = nullptr;
+  if (na < 0 || navel < na)
+    return fail(EVP1D_ERR_INVALID_ARG, "need 0 <= na <= navel (na=%d navel=%d)",
+                na, navel);
+  if (!params) return fail(EVP1D_ERR_INVALID_ARG, "params is NULL");
+  const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
+  const double *geo[7] = {dxT, dyT, HTE, HTN, HTEm1, HTNm1, uarear};
+  if (na > 0) {
+    if (!nonnull_all((const void *const *)idx, 6))
+      return fail(EVP1D_ERR_INVALID_ARG, "a neighbour vector is NULL");
+    if (!nonnull_all((const void *const *)geo, 7))
+      return fail(EVP1D_ERR_INVALID_ARG, "a geometry field is NULL");
+  }
+  // Host-side validation: every neighbour index must address a slot in
+  // 1..navel, so no device gather can leave its buffer.
+  CHECK(validate_neighbours(na, navel, idx, -1));
+  return init_common(handle, na, navel, idx, geo, params, device);
+}
+
+int evp1d_init_batched(evp1d_t **handle, int nmembers, const int32_t *na_m,
+                       const int32_t *navel_m, const int32_t *ee, const int32_t *ne,
+                       const int32_t *se, const int32_t *nw, const int32_t *sw,
+                       const int32_t *sse, const double *dxT, const double *dyT,
+                       const double *HTE, const double *HTN, const double *HTEm1,
+                       const double *HTNm1, const double *uarear,
+                       const evp1d_params *params, int device) {
+  g_err.clear();
+  if (!handle) return fail(EVP1D_ERR_INVALID_ARG, "handle is NULL");
+  *handle = nullptr;
+  if (nmembers < 1 || !na_m || !navel_m || !params)
+    return fail(EVP1D_ERR_INVALID_ARG, "need nmembers >= 1, na, navel and params");
+  long long NA = 0, NV = 0;
+  for (int m = 0; m < nmembers; m++) {
+    if (na_m[m] < 0 || navel_m[m] < na_m[m])
+      return fail(EVP1D_ERR_INVALID_ARG, "member %d: need 0 <= na <= navel", m);
+    NA += na_m[m];
+    NV += navel_m[m];
+  }
+  if (NV > 0x7fffffffLL) return fail(EVP1D_ERR_INVALID_ARG, "ensemble too large for int32");
+  const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
+  const double *geo[7] = {dxT, dyT, HTE, HTN, HTEm1, HTNm1, uarear};
+  if (NA > 0) {
+    if (!nonnull_all((const void *const *)idx, 6))
+      return fail(EVP1D_ERR_INVALID_ARG, "a neighbour vector is NULL");
+    if (!nonnull_all((const void *const *)geo, 7))
+      return fail(EVP1D_ERR_INVALID_ARG, "a geometry field is NULL");
+  }
+  // combined 1-based index space: all members' list points, then all halos
+  std::vector<int32_t> comb((size_t)NA * 6);
+  std::vector<int64_t> uv_pos((size_t)NV);
+  long long lo = 0, ho = 0, co = 0;  // list offset, halo offset, caller offset
+  for (int m = 0; m < nmembers; m++) {
+    const int n = na_m[m], nv = navel_m[m];
+    const int32_t *mi[6];
+    for (int k = 0; k < 6; k++) mi[k] = idx[k] + lo;
+    CHECK(validate_neighbours(n, nv, mi, m));
+    for (int k = 0; k < 6; k++)
+      for (int w = 0; w < n; w++) {
+        const int32_t v = mi[k][w];
+        comb[(size_t)k * NA + lo + w] = (int32_t)(v <= n ? lo + v : NA + ho + (v - n));
+      }
+    for (int w = 0; w < n; w++) uv_pos[lo + w] = co + w;
+    for (int w = 0; w < nv - n; w++) uv_pos[NA + ho + w] = co + n + w;
+    lo += n;
+    ho += nv - n;
+    co += nv;
+  }
+  const int32_t *cidx[6];
+  for (int k = 0; k < 6; k++) cidx[k] = comb.data() + (size_t)k * NA;
+  CHECK(init_common(handle, (int)NA, (int)NV, cidx, geo, params, device));
+  (*handle)->nmembers = nmembers;
+  (*handle)->uv_pos = std::move(uv_pos);
   return EVP1D_OK;
 }
 
@@ -292,7 +419,13 @@ int evp1d_set_params(evp1d_t *h, const evp1d_params *params) {
 int evp1d_upload(evp1d_t *h, const evp1d_fields *io) {
   if (!h || !io) return fail(EVP1D_ERR_INVALID_ARG, "NULL argument");
   CHECK(select_device(h));
-  CHECK(evp::problem_upload(&h->d, io, h->p.rhow));
+  if (h->nmembers > 1 && h->d.na > 0) {
+    if (!io->uvel || !io->vvel) return fail(EVP1D_ERR_INVALID_ARG, "uvel/vvel are NULL");
+    const evp1d_fields c = combined_view(h, io, true);
+    CHECK(evp::problem_upload(&h->d, &c, h->p.rhow));
+  } else {
+    CHECK(evp::problem_upload(&h->d, io, h->p.rhow));
+  }
   h->uploaded = true;
   return EVP1D_OK;
 }
@@ -329,6 +462,13 @@ int evp1d_download(evp1d_t *h, const evp1d_fields *io) {
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "nothing uploaded");
   CHECK(select_device(h));
   CHECK(check_device_error(h));
+  if (h->nmembers > 1 && h->d.na > 0) {
+    if (!io->uvel || !io->vvel) return fail(EVP1D_ERR_INVALID_ARG, "uvel/vvel are NULL");
+    const evp1d_fields c = combined_view(h, io, false);
+    CHECK(evp::problem_download(&h->d, &c));
+    scatter_combined(h, io, h->d.na);
+    return EVP1D_OK;
+  }
   return evp::problem_download(&h->d, io);
 }
 
@@ -378,6 +518,97 @@ int evp1d_debug_trace(evp1d_t *h, long long *out, int n) {
   CHECK(select_device(h));
   CUDA_TRY(cudaStreamSynchronize(h->d.stream));
   CUDA_TRY(cudaMemcpy(out, h->trace, sizeof(long long) * (size_t)n, cudaMemcpyDeviceToHost));
+  return EVP1D_OK;
+}
+
+int evp1d_autotune(evp1d_t *h, int nsub, char *chosen, int len) {
+  if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
+  if (nsub < 1) return fail(EVP1D_ERR_INVALID_ARG, "nsub = %d < 1", nsub);
+  if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");
+  CHECK(select_device(h));
+  DeviceProblem &d = h->d;
+  if (d.ntiles == 0) return EVP1D_OK;
+  cudaStream_t st = d.stream;
+  // every array a trial writes: both state buffers, outputs, str
+  std::vector<std::pair<double *, size_t>> arrs;
+  for (int b = 0; b < 2; b++) {
+    for (int k = 0; k < 12; k++) arrs.push_back({d.stress[b][k], (size_t)d.nslots});
+    arrs.push_back({d.u[b], (size_t)d.nuv});
+    arrs.push_back({d.v[b], (size_t)d.nuv});
+  }
+  arrs.push_back({d.strintx, (size_t)d.nslots});
+  arrs.push_back({d.strinty, (size_t)d.nslots});
+  arrs.push_back({d.Cb, (size_t)d.nslots});
+  for (int k = 0; k < 8; k++) arrs.push_back({d.str[k], (size_t)d.nuv});
+  size_t total = 0;
+  for (auto &a : arrs) total += a.second;
+  double *backup = nullptr;
+  CUDA_TRY(cudaMalloc(&backup, total * sizeof(double)));
+  auto copy_all = [&](bool save) {
+    size_t o = 0;
+    for (auto &a : arrs) {
+      if (save)
+        cudaMemcpyAsync(backup + o, a.first, a.second * sizeof(double), cudaMemcpyDeviceToDevice, st);
+      else
+        cudaMemcpyAsync(a.first, backup + o, a.second * sizeof(double), cudaMemcpyDeviceToDevice, st);
+      o += a.second;
+    }
+  };
+  const int cur0 = d.cur;
+  copy_all(true);
+  struct Cand {
+    int path, prefetch;
+  };
+  const Cand cands[] = {{kPathTma, 0}, {kPathTma, 2}, {kPathFused, 0}};
+  const int old_path = h->path, old_pf = h->prefetch;
+  int best = -1;
+  float best_ms = 0.f;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int rc = EVP1D_OK;
+  for (int c = 0; c < 3 && rc == EVP1D_OK; c++) {
+    h->path = cands[c].path;
+    h->prefetch = cands[c].prefetch;
+    drop_graphs(h);
+    rc = evp1d_subcycles(h, 2);  // warm-up (also builds nothing: < one chunk)
+    if (rc != EVP1D_OK) break;
+    cudaEventRecord(e0, st);
+    rc = evp1d_subcycles(h, nsub);
+    cudaEventRecord(e1, st);
+    if (rc != EVP1D_OK) break;
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (best < 0 || ms < best_ms) {
+      best = c;
+      best_ms = ms;
+    }
+    copy_all(false);
+    d.cur = cur0;
+  }
+  cudaStreamSynchronize(st);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(backup);
+  drop_graphs(h);
+  if (rc != EVP1D_OK || best < 0) {
+    h->path = old_path;
+    h->prefetch = old_pf;
+    return rc != EVP1D_OK ? rc : fail(EVP1D_ERR_CUDA, "autotune found no candidate");
+  }
+  CHECK(check_device_error(h));
+  h->path = cands[best].path;
+  h->prefetch = cands[best].prefetch;
+  char buf[128];
+  snprintf(buf, sizeof buf, "%s prefetch=%d (%.2f us/subcycle)",
+           h->path == kPathTma ? "fused-tile-tma" : "fused-tile", h->prefetch,
+           1000.0 * best_ms / nsub);
+  h->tuned = buf;
+  if (chosen && len > 0) {
+    strncpy(chosen, buf, (size_t)len - 1);
+    chosen[len - 1] = 0;
+  }
   return EVP1D_OK;
 }
 

@@ -180,6 +180,40 @@ class EVP1D:
         self.h = h
 
     @classmethod
+    def batched(cls, ens, ndte: int = None, params: Params = None,
+                device: int = 0) -> "EVP1D":
+        """An ensemble handle (evp1d_init_batched) for a
+        :class:`evp1d.synth.Ensemble`; FieldSets for it are built from
+        ``ens.combined``."""
+        L = _lib.load()
+        pr = ens.combined
+        if params is None:
+            params = set_evp_parameters(ndte if ndte is not None else pr.ndte)
+        f = pr.f
+        idx = [_as_i32(pr.idx[k], pr.na, k) for k in ("ee", "ne", "se", "nw", "sw", "sse")]
+        geo = [_as_f64(f[k], pr.na, k) for k in ("dxT", "dyT", "HTE", "HTN", "HTEm1", "HTNm1", "uarear")]
+        na = np.ascontiguousarray(ens.na, dtype=np.int32)
+        navel = np.ascontiguousarray(ens.navel, dtype=np.int32)
+        h = C.c_void_p()
+        rc = L.evp1d_init_batched(C.byref(h), len(na), na.ctypes.data_as(_I),
+                                  navel.ctypes.data_as(_I),
+                                  *[a.ctypes.data_as(_I) for a in idx],
+                                  *[a.ctypes.data_as(_D) for a in geo],
+                                  C.byref(params), int(device))
+        check(rc, "evp1d_init_batched")
+        self = cls.__new__(cls)
+        self._L, self.h, self.params = L, h, params
+        self.na, self.navel = pr.na, pr.navel
+        return self
+
+    def autotune(self, nsub: int = 20) -> str:
+        """Pick the fastest kernel variant on the uploaded state
+        (evp1d_autotune); returns the choice."""
+        buf = C.create_string_buffer(128)
+        check(self._L.evp1d_autotune(self.h, int(nsub), buf, 128), "evp1d_autotune")
+        return buf.value.decode()
+
+    @classmethod
     def from_problem(cls, prob, ndte: int = None, params: Params = None,
                      device: int = 0) -> "EVP1D":
         f = prob.f

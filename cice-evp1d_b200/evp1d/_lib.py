@@ -86,6 +86,11 @@ def load() -> C.CDLL:
     L.evp1d_last_error.restype = C.c_char_p
     L.evp1d_last_error.argtypes = []
     L.evp1d_version.restype = C.c_char_p
+    L.evp1d_init_batched.argtypes = ([C.POINTER(H), C.c_int, _I, _I] + [_I] * 6
+                                     + [_D] * 7 + [C.POINTER(Params), C.c_int])
+    L.evp1d_init_batched.restype = C.c_int
+    L.evp1d_autotune.argtypes = [H, C.c_int, C.c_char_p, C.c_int]
+    L.evp1d_autotune.restype = C.c_int
     L.evp1d_debug_trace.argtypes = [H, C.POINTER(C.c_longlong), C.c_int]
     L.evp1d_debug_trace.restype = C.c_int
     L.evp1d_kernel_path.argtypes = [H]

@@ -302,3 +302,48 @@ def make_ensemble(n_members: int, ny: int, nx_lo: int, nx_hi: int, seed: int,
                       strength_scale=float(scales[m]), forcing_sd=0.02)
         out.append(to_1d(g))
     return out
+
+
+@dataclass
+class Ensemble:
+    """Members concatenated member-major, the layout of evp1d_init_batched:
+    per-point arrays back to back, u/v with each member's halo slots after its
+    own list points, neighbour vectors 1-based within each member."""
+
+    members: list
+    combined: Problem1D   # na = sum(na), navel = sum(navel); idx member-local
+    na: np.ndarray        # [nmembers] int32
+    navel: np.ndarray     # [nmembers] int32
+
+    def split_points(self, a: np.ndarray) -> list:
+        """Per-member views of a concatenated per-point array ([..., sum(na)])."""
+        o = np.concatenate([[0], np.cumsum(self.na)])
+        return [a[..., o[m]:o[m + 1]] for m in range(len(self.members))]
+
+    def split_slots(self, a: np.ndarray) -> list:
+        """Per-member views of a concatenated u/v/str array ([..., sum(navel)])."""
+        o = np.concatenate([[0], np.cumsum(self.navel)])
+        return [a[..., o[m]:o[m + 1]] for m in range(len(self.members))]
+
+
+def concat(members: list) -> Ensemble:
+    na = np.array([m.na for m in members], dtype=np.int32)
+    navel = np.array([m.navel for m in members], dtype=np.int32)
+    cat = lambda xs: np.concatenate(xs) if xs else np.zeros(0)
+    f = {k: cat([m.f[k] for m in members]) for k in members[0].f}
+    idx = {k: cat([m.idx[k] for m in members]).astype(np.int32) for k in members[0].idx}
+    comb = Problem1D(
+        na=int(na.sum()), navel=int(navel.sum()), ndte=members[0].ndte, idx=idx,
+        skipT=cat([m.skipT for m in members]).astype(np.int32),
+        skipU=cat([m.skipU for m in members]).astype(np.int32), f=f,
+        stress=np.concatenate([m.stress for m in members], axis=1),
+        uvel=cat([m.uvel for m in members]), vvel=cat([m.vvel for m in members]),
+        strintx=cat([m.strintx for m in members]), strinty=cat([m.strinty for m in members]),
+        Cb=cat([m.Cb for m in members]))
+    return Ensemble(members=members, combined=comb, na=na, navel=navel)
+
+
+# Ensemble configurations (uneven member domains).
+ENSEMBLES = {
+    "cfg3": dict(n_members=64, ny=300, nx_lo=100, nx_hi=1300, seed=3, ndte=500),
+}

@@ -109,6 +109,30 @@ int evp1d_init(evp1d_t **handle, int na, int navel, const int32_t *ee,
                const double *HTEm1, const double *HTNm1, const double *uarear,
                const evp1d_params *params, int device);
 
+/* An ensemble of independent 1D problems (members) solved together: one
+ * tile plan over all members, one kernel launch per subcycle for the whole
+ * ensemble.  Member m has na[m] list points and navel[m] slots; its neighbour
+ * vectors are 1-based within the member.  Every array argument here and in
+ * the evp1d_fields of later calls is the member-major concatenation of the
+ * members' arrays (per-point fields: sum(na) entries; uvel, vvel, str:
+ * sum(navel) entries, each member's halo slots after its own list points).
+ * Results are bitwise those of solving each member alone.  No counterpart in
+ * the reference, which solves one state per call. */
+int evp1d_init_batched(evp1d_t **handle, int nmembers, const int32_t *na,
+                       const int32_t *navel, const int32_t *ee,
+                       const int32_t *ne, const int32_t *se, const int32_t *nw,
+                       const int32_t *sw, const int32_t *sse,
+                       const double *dxT, const double *dyT, const double *HTE,
+                       const double *HTN, const double *HTEm1,
+                       const double *HTNm1, const double *uarear,
+                       const evp1d_params *params, int device);
+
+/* Time the kernel variants (TMA-fed with and without L2 prefetch, plain
+ * loads) for `nsub` subcycles on the uploaded state, keep the fastest for
+ * this handle and restore the state.  `chosen` (may be NULL) receives a
+ * description of the choice.  Needs a prior evp1d_upload. */
+int evp1d_autotune(evp1d_t *handle, int nsub, char *chosen, int len);
+
 /* Release the handle and its device buffers (dyn_evp1d_finalize,
  * integration/ice_dyn_evp1d.F90:326-331).  NULL is a no-op. */
 int evp1d_finalize(evp1d_t *handle);

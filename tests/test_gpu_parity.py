@@ -273,3 +273,47 @@ def test_shortcut_edges(oracle_mod, u0):
     p.u0 = u0
     fs = gpu_run(pr, 7, params=p)
     assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 7, params=p), pr)
+
+
+def test_golden_fixture_md5():
+    """The CUDA path reproduces the committed fixture's md5s and arrays."""
+    import golden_io
+    pr, out, exp = golden_io.load()
+    fs = gpu_run(pr, pr.ndte)
+    f1, f2 = helpers.output_files(fs.stress, fs.strintx, fs.strinty, fs.uvel, fs.vvel, pr.skipU)
+    assert helpers.md5(f1) == exp["md5_stress_v2"]
+    assert helpers.md5(f2) == exp["md5_stepu_v2"]
+    assert np.array_equal(fs.str.view(np.int64), out["str"].view(np.int64))
+
+
+def test_batched_ensemble_matches_members(oracle_mod):
+    """Uneven members solved in one handle give, member by member, bitwise the
+    single-member results (and the oracle's)."""
+    members = [synth.make_problem("cfg1", nx=nx, ny=ny, seed=40 + i, ndte=8)
+               for i, (nx, ny) in enumerate([(30, 20), (75, 41), (12, 9), (50, 60), (90, 17)])]
+    ens = synth.concat(members)
+    fs = evp1d.FieldSet.from_problem(ens.combined, want_str=True)
+    with evp1d.EVP1D.batched(ens, ndte=8) as s:
+        s.run(8, fs)
+    for m, pr in enumerate(members):
+        st = oracle_run(oracle_mod, pr, 8)
+        one = evp1d.FieldSet(pr.na, pr.navel, skipT=pr.skipT, skipU=pr.skipU,
+                             stress=ens.split_points(fs.stress)[m],
+                             uvel=ens.split_slots(fs.uvel)[m], vvel=ens.split_slots(fs.vvel)[m],
+                             strintx=ens.split_points(fs.strintx)[m],
+                             strinty=ens.split_points(fs.strinty)[m], Cb=ens.split_points(fs.Cb)[m],
+                             want_str=True, **{k: pr.f[k] for k in evp1d.FieldSet.DYN})
+        one.str[:] = ens.split_slots(fs.str)[m]
+        assert_same(one, st, pr)
+
+
+def test_autotune_keeps_state(oracle_mod):
+    pr = synth.make_problem("cfg1", nx=120, ny=90, ndte=12)
+    fs = evp1d.FieldSet.from_problem(pr, want_str=True)
+    with evp1d.EVP1D.from_problem(pr, ndte=12) as s:
+        s.upload(fs)
+        choice = s.autotune(6)
+        assert "us/subcycle" in choice
+        s.subcycles(12)
+        s.download(fs)
+    assert_same(fs, oracle_run(oracle_mod, pr, 12), pr)
