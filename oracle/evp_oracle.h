@@ -16,12 +16,14 @@
  * copysign).  Built with -ffp-contract=off -fno-fast-math this matches the
  * reference's f0/f1 (-fp-model precise -no-fma) semantics.
  *
- * Parity pinning: the reference's only golden vectors are md5 sums over DMI
- * input files that are not distributed (README.md:63-104).  This oracle is
- * pinned by the reference's own acceptance criterion instead -- the v0 2D form
- * and the v2 1D form must produce md5-identical output files on the same input
- * -- plus analytic known answers derived from the integration smoke test
- * configuration (integration/ice_dyn_evp1d_standalone.F90:60-79).
+ * Parity unpinned against the reference's own outputs: its only golden
+ * vectors are md5 sums over DMI input files that are not distributed
+ * (README.md:63-104), and the Fortran reference cannot be compiled in this
+ * image.  The oracle is held instead by the reference's own acceptance
+ * criterion -- the v0 2D form and the v2 1D form produce md5-identical output
+ * files on the same input -- by closed-form answers of the integration smoke
+ * test state (integration/ice_dyn_evp1d_standalone.F90:60-79), and by the
+ * committed fixture in tests/golden.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline may use
  * this code.  The product path never links it.
