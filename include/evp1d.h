@@ -201,6 +201,39 @@ int evp1d_build_index(int nx, int ny, int nghost, const int32_t *mask,
                       int32_t *sw, int32_t *sse);
 
 /* ----------------------------------------------------------------------------
+ * 2D adapter: dyn_evp1d_init / dyn_evp1d_run / dyn_evp1d_finalize on global
+ * 2D arrays (integration/ice_dyn_evp1d.F90:65-255, 326-331).  Arrays are
+ * [nx*ny] column-major (i fastest) including the ghost cells, nx = nx_global
+ * + 2*nghost as the adapter's G_* arrays (:93-94).  init builds the 1D list
+ * from tmask (:559-589, 743-816); run derives skipT/skipU from the ice masks
+ * (set_skipMe, :521-537), gathers the fields onto the list with halo
+ * velocities 0 (convert_2d_1d_dyn, :818-882), runs ndte subcycles on the GPU
+ * and scatters the results back (convert_1d_2d_dyn, :884-947).  Unlike the
+ * reference, whose L_* arguments are intent(in), results are returned in the
+ * inout arrays.
+ * -------------------------------------------------------------------------- */
+typedef struct evp1d_dyn_fields {
+  double *stress[12];          /* inout: stressp_1..4, stressm_1..4, stress12_1..4 */
+  const double *strength;      /* in */
+  const double *cdn_ocn, *aiu, *uocn, *vocn, *waterxU, *wateryU;  /* in */
+  const double *forcexU, *forceyU, *umassdti, *fmU, *Tbu;          /* in */
+  double *strintxU, *strintyU, *Cb;  /* inout: written at ice U points */
+  double *uvel, *vvel;               /* inout */
+  const int32_t *icetmask, *iceumask;  /* in, nonzero = ice */
+} evp1d_dyn_fields;
+
+typedef struct evp1d_dyn_handle evp1d_dyn_t;
+
+int evp1d_dyn_init(evp1d_dyn_t **handle, int nx, int ny, int nghost,
+                   const int32_t *tmask, const double *dyT, const double *dxT,
+                   const double *uarear, const double *HTE, const double *HTN,
+                   const evp1d_params *params, int device);
+int evp1d_dyn_run(evp1d_dyn_t *handle, int ndte, const evp1d_dyn_fields *io);
+int evp1d_dyn_finalize(evp1d_dyn_t *handle);
+/* Number of 1D list points (nActive) and slots (navel) of a 2D handle. */
+int evp1d_dyn_sizes(evp1d_dyn_t *handle, int *na, int *navel);
+
+/* ----------------------------------------------------------------------------
  * Host-only diagnostics of the tile plan the solver would build for a 1D
  * problem (same arguments as evp1d_init, 1-based neighbours; no GPU needed).
  * stats[0] tiles, [1] device slots (list points + alignment padding),

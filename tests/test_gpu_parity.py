@@ -317,3 +317,53 @@ def test_autotune_keeps_state(oracle_mod):
         s.subcycles(12)
         s.download(fs)
     assert_same(fs, oracle_run(oracle_mod, pr, 12), pr)
+
+
+def test_reference_file_case_on_gpu(tmp_path):
+    """A case in the reference's file formats, run on the GPU, reproduces the
+    golden fixture's md5 sums (python -m evp1d.io)."""
+    import golden_io
+    from evp1d import io as evio
+    pr, _, exp = golden_io.load()
+    p = evp1d.set_evp_parameters(pr.ndte)
+    evio.write_inputs(str(tmp_path), pr, dict(capping=p.capping, e_factor=p.e_factor,
+                                              epp2i=p.epp2i, deltaminEVP=p.deltaminEVP))
+    h = evio.run_case(str(tmp_path), pr.na, pr.navel, pr.ndte)
+    assert h == (exp["md5_stress_v2"], exp["md5_stepu_v2"])
+
+
+@pytest.mark.parametrize("curvilinear", [False, True])
+def test_dyn2d_adapter_matches_v0(oracle_mod, curvilinear):
+    """The 2D adapter (list = every ocean point, skip flags from the ice masks,
+    as dyn_evp1d_init/run) against the oracle's v0 2D kernels (upstream CICE
+    form): bitwise equal stresses, velocities and internal stress divergence."""
+    from evp1d import dyn
+    g = synth.make_grid(64, 50, seed=17, ndte=9, curvilinear=curvilinear)
+    p = evp1d.set_evp_parameters(9)
+    F = dyn.fields_from_grid(g)
+    with dyn.Dyn2D(g.tmask, g.f["dyT"], g.f["dxT"], g.f["uarear"], g.f["HTE"],
+                   g.f["HTN"], p) as d:
+        na, navel = d.sizes
+        assert na == int(g.tmask.sum())
+        d.run(9, F, g.iceT, g.iceU)
+    V = oracle_mod.run_v0(g, 9)
+    for k in dyn.STRESS:
+        assert np.array_equal(F[k].view(np.int64), V[k].view(np.int64)), k
+    for mine, ref in (("uvel", "uvel"), ("vvel", "vvel"), ("strintxU", "strintx"),
+                      ("strintyU", "strinty")):
+        assert np.array_equal(F[mine].view(np.int64), V[ref].view(np.int64)), mine
+
+
+def test_sharded_run_single_rank_gpu(oracle_mod):
+    """The ensemble driver on one rank (no process group) solves its members
+    on the GPU with the same summaries as the oracle."""
+    from evp1d import ensemble
+    members = [synth.make_problem("cfg1", nx=nx, ny=25, seed=90 + i, ndte=5)
+               for i, nx in enumerate([20, 47, 33])]
+    got = ensemble.sharded_run(members, 5)
+    for i, pr in enumerate(members):
+        st = oracle_run(oracle_mod, pr, 5)
+        want = ensemble.summarize(dict(stress=st.stress, uvel=st.uvel[: pr.navel],
+                                       vvel=st.vvel[: pr.navel], strintx=st.strintx,
+                                       strinty=st.strinty, Cb=st.Cb), pr.na)
+        assert got[i] == want
