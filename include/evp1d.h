@@ -245,6 +245,46 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
                      const int32_t *se, const int32_t *nw, const int32_t *sw,
                      const int32_t *sse, long long stats[8]);
 
+/* ----------------------------------------------------------------------------
+ * Allocation-free entry point.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory -- device memory owned by
+ * another runtime or memory pool, or code where a cudaMalloc would
+ * synchronise the device or fail -- and that already hold the 1D problem in
+ * device memory.  One call runs ndte x {stress; stepu} in place on the
+ * caller's device arrays in the reference 1D layout, exactly as evp1d_run
+ * does on host arrays, with the reference-order stress and stepu kernels.
+ *
+ * - Every pointer (neighbours, geometry, every field of `io`) is device (or
+ *   managed) memory of the calling thread's current device; neighbours are
+ *   1-based as in evp1d_init; skipT/skipU nonzero = skip.  uvel_init/
+ *   vvel_init may both be NULL (= the velocities at call start); str[k] may be
+ *   NULL (str1..str8 are then not returned).
+ * - The call allocates nothing.  str1..str8 and the call-start velocities
+ *   live in one fixed device array of the library holding navel up to
+ *   EVP1D_NOALLOC_MAX_NAVEL (10 arrays of that many doubles, 20 MiB);
+ *   a larger navel is rejected with EVP1D_ERR_INVALID_ARG.
+ * - str1..str8 are cleared at the start of every call.  Every call on a
+ *   device shares that array, so calls that overlap on the GPU (from several
+ *   host threads, or on streams that run concurrently) race; serialise them.
+ * - The first call with a device current looks up the array's device
+ *   address; make that first call before any stream capture.
+ * - Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
+ *   stream) and the call returns after the stream has finished it.
+ *   Neighbours outside 1..navel give EVP1D_ERR_INDEX before any array is
+ *   written.
+ * -------------------------------------------------------------------------- */
+#define EVP1D_NOALLOC_MAX_NAVEL 262144
+int evp1d_run_device_noalloc(int na, int navel, const int32_t *ee,
+                             const int32_t *ne, const int32_t *se,
+                             const int32_t *nw, const int32_t *sw,
+                             const int32_t *sse, const double *dxT,
+                             const double *dyT, const double *HTE,
+                             const double *HTN, const double *HTEm1,
+                             const double *HTNm1, const double *uarear,
+                             const evp1d_params *params, int ndte,
+                             const evp1d_fields *io, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
