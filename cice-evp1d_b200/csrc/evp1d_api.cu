@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "evp1d.h"
+#include "evp_handle.h"
 #include "evp_internal.h"
 
 using evp::DevState;
@@ -72,27 +73,6 @@ Params to_params(const evp1d_params &q) {
 constexpr int kGraphChunk = 50;
 
 }  // namespace
-
-// Kernel paths of the fused subcycle.
-enum { kPathTma = 0, kPathFused = 1 };
-
-struct evp1d_handle {
-  DeviceProblem d;
-  Params p{};
-  int path = kPathTma;
-  int prefetch = 0;  // L2 prefetch distance of the TMA kernel (tiles)
-  long long *trace = nullptr;  // device timing trace (EVP1D_TRACE, debug)
-  bool uploaded = false;
-  long long launches = 0;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // by starting buffer
-  // ensemble (batched) handles: caller arrays are member-major concatenations
-  // with each member's halo slots after its list points; uv_pos maps the
-  // combined slot order (all list points, then all halo slots) to them.
-  int nmembers = 1;
-  std::vector<int64_t> uv_pos;
-  std::vector<double> uv_tmp;  // scratch for u, v (and str) in combined order
-  std::string tuned;           // last autotuner choice
-};
 
 namespace {
 
@@ -396,6 +376,7 @@ int evp1d_finalize(evp1d_t *h) {
   if (!h) return EVP1D_OK;
   cudaSetDevice(h->d.device);
   drop_graphs(h);
+  evp::adjoint_release(h->adj);
   evp::problem_destroy(&h->d);
   if (h->trace) cudaFree(h->trace);
   delete h;
@@ -408,6 +389,7 @@ int evp1d_set_params(evp1d_t *h, const evp1d_params *params) {
   const double old_rhow = h->p.rhow;
   h->p = to_params(*params);
   drop_graphs(h);
+  evp::adjoint_invalidate(h->adj);
   if (h->uploaded && h->p.rhow != old_rhow && h->d.nslots > 0) {
     evp::launch_drag_factor(h->d.nslots, h->d.dyn[evp::kAiu], h->d.dyn[evp::kCw],
                             h->p.rhow, h->d.dyn[evp::kKvrel], h->d.stream);
@@ -419,6 +401,8 @@ int evp1d_set_params(evp1d_t *h, const evp1d_params *params) {
 int evp1d_upload(evp1d_t *h, const evp1d_fields *io) {
   if (!h || !io) return fail(EVP1D_ERR_INVALID_ARG, "NULL argument");
   CHECK(select_device(h));
+  evp::adjoint_invalidate(h->adj);
+  h->uinit_explicit = io->uvel_init != nullptr;
   if (h->nmembers > 1 && h->d.na > 0) {
     if (!io->uvel || !io->vvel) return fail(EVP1D_ERR_INVALID_ARG, "uvel/vvel are NULL");
     const evp1d_fields c = combined_view(h, io, true);

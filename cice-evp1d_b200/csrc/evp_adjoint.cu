@@ -1,0 +1,753 @@
+// evp_adjoint.cu -- reverse-mode gradients of the EVP subcycle loop.
+//
+// Forward (recording) pass: the ordinary fused subcycles, saving either
+//  - every subcycle's velocities (a full velocity tape, when it fits the
+//    device memory budget), or
+//  - (u, v, 12 stresses) every `interval` subcycles (checkpoints).
+// Reverse sweep, subcycle n = ndte-1 .. 0, in the solver's slot order:
+//  - checkpoint mode first recomputes the velocities of one segment from its
+//    checkpoint with the forward kernel into a segment tape;
+//  - k_adj_stepu: per U point, the velocity adjoint lam_u(n+1) is completed
+//    by gathering the stress kernel's corner contributions, then stepu is
+//    reversed (src/bench_v2b.F90:509-544): lam_u(n) through stepu, the
+//    adjoint of strintx/strinty scaled by uarear, and the forcex, forcey and
+//    Cw gradients;
+//  - k_adj_stress: per T point, the str adjoints are gathered from the U
+//    points that read them (nw/sse/sw transposed), str_combine, the corner
+//    relaxations and the strain rates are reversed (src/bench_v2b.F90:
+//    137-310, 363-437); the stress adjoint is updated in place and the
+//    strength gradient accumulated.
+// Every neighbour access of the reverse sweep is a gather through transposed
+// neighbour lists built once per handle, so the sweep uses no atomics and is
+// deterministic.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "evp1d.h"
+#include "evp_adjoint_math.cuh"
+#include "evp_handle.h"
+#include "evp_internal.h"
+
+namespace evp {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+#define ADJ_TRY(x)                                                         \
+  do {                                                                     \
+    cudaError_t e_ = (x);                                                  \
+    if (e_ != cudaSuccess)                                                 \
+      return error(e_ == cudaErrorMemoryAllocation ? EVP1D_ERR_NOMEM       \
+                                                   : EVP1D_ERR_CUDA,       \
+                   "%s: %s", #x, cudaGetErrorString(e_));                  \
+  } while (0)
+
+#define ADJ_CHECK(x)                \
+  do {                              \
+    int rc_ = (x);                  \
+    if (rc_ != EVP1D_OK) return rc_; \
+  } while (0)
+
+// Transposed neighbour lists (CSR over slots).
+enum {
+  kTrNw = 0,   // U points x with nw(x) = w   (they read str2, str7 at w)
+  kTrSse = 1,  // U points x with sse(x) = w  (str3, str6)
+  kTrSw = 2,   // U points x with sw(x) = w   (str4, str8)
+  kTrEe = 3,   // T points w with ee(w) = x   (they read u, v at x as "ee")
+  kTrNe = 4,   // T points w with ne(w) = x
+  kTrSe = 5,   // T points w with se(w) = x
+  kNumTr = 6
+};
+enum { kGStrength, kGCw, kGForcex, kGForcey, kGUinit, kGVinit, kNumGrad };
+
+struct AdjArgs {
+  int nslots = 0;
+  const uint8_t *flags = nullptr;
+  const int32_t *ee = nullptr, *ne = nullptr, *se = nullptr;
+  const int32_t *tr_off[kNumTr] = {}, *tr_idx[kNumTr] = {};
+  const double *dxT = nullptr, *dyT = nullptr, *HTE = nullptr, *HTN = nullptr;
+  const double *HTEm1 = nullptr, *HTNm1 = nullptr, *uarear = nullptr;
+  const double *strength = nullptr, *kvrel = nullptr, *aiu = nullptr;
+  const double *uocn = nullptr, *vocn = nullptr, *waterx = nullptr, *watery = nullptr;
+  const double *umassdti = nullptr, *fm = nullptr, *Tbu = nullptr;
+  double *Pu = nullptr, *Pv = nullptr;  // lam of u, v through stepu alone
+  double *Lx = nullptr, *Ly = nullptr;  // uarear * lam of strintx, strinty
+  double *C8[8] = {};                   // lam of the 8 corner velocities of a T point
+  double *LS[12] = {};                  // lam of the 12 stresses
+  double *g[kNumGrad] = {};
+};
+
+// lam of u(n+1), v(n+1) at x: stepu's own part plus the stress corners that
+// read the velocity at x (as cc of x, and as ee/ne/se of other T points).
+__device__ __forceinline__ void velocity_lam(const AdjArgs &a, int x, double &lu,
+                                             double &lv) {
+  lu = a.Pu[x] + a.C8[0][x];
+  lv = a.Pv[x] + a.C8[1][x];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int32_t *off = a.tr_off[kTrEe + k], *idx = a.tr_idx[kTrEe + k];
+    const int b = off[x], e = off[x + 1];
+    for (int q = b; q < e; q++) {
+      const int w = idx[q];
+      lu += a.C8[2 + 2 * k][w];
+      lv += a.C8[3 + 2 * k][w];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__restrict__ v0,
+            const double *__restrict__ u1, const double *__restrict__ v1) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.nslots;
+       x += gridDim.x * blockDim.x) {
+    double lu, lv;
+    velocity_lam(a, x, lu, lv);
+    if (a.flags[x] & kSkipU) {  // u(n+1) = u(n) here
+      a.Pu[x] = lu;
+      a.Pv[x] = lv;
+      a.Lx[x] = 0.0;
+      a.Ly[x] = 0.0;
+      continue;
+    }
+    StepuAdjIn in;
+    in.uold = u0[x];
+    in.vold = v0[x];
+    in.unew = u1[x];
+    in.vnew = v1[x];
+    in.lun = lu;
+    in.lvn = lv;
+    in.kvrel = a.kvrel[x];
+    in.aiXrhow = a.aiu[x] * p.rhow;
+    in.uocn = a.uocn[x];
+    in.vocn = a.vocn[x];
+    in.waterx = a.waterx[x];
+    in.watery = a.watery[x];
+    in.umassdti = a.umassdti[x];
+    in.fm = a.fm[x];
+    in.Tbu = a.Tbu[x];
+    const StepuAdjOut o = stepu_adjoint(in, p);
+    a.Pu[x] = o.luold;
+    a.Pv[x] = o.lvold;
+    const double ar = a.uarear[x];
+    a.Lx[x] = ar * o.lcc1;
+    a.Ly[x] = ar * o.lcc2;
+    a.g[kGForcex][x] += o.lcc1;
+    a.g[kGForcey][x] += o.lcc2;
+    a.g[kGCw][x] += o.gCw;
+    if (p.revp != 0.0) {
+      a.g[kGUinit][x] += o.luinit;
+      a.g[kGVinit][x] += o.lvinit;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__restrict__ v) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < a.nslots;
+       w += gridDim.x * blockDim.x) {
+    if (a.flags[w] & kSkipT) {  // stresses unchanged, str not written
+#pragma unroll
+      for (int k = 0; k < 8; k++) a.C8[k][w] = 0.0;
+      continue;
+    }
+    double lo[8];
+    lo[0] = a.Lx[w];
+    lo[4] = a.Ly[w];
+    {
+      const int32_t *off = a.tr_off[kTrNw], *idx = a.tr_idx[kTrNw];
+      double sx = 0.0, sy = 0.0;
+      for (int q = off[w]; q < off[w + 1]; q++) {
+        sx += a.Lx[idx[q]];
+        sy += a.Ly[idx[q]];
+      }
+      lo[1] = sx;
+      lo[6] = sy;
+    }
+    {
+      const int32_t *off = a.tr_off[kTrSse], *idx = a.tr_idx[kTrSse];
+      double sx = 0.0, sy = 0.0;
+      for (int q = off[w]; q < off[w + 1]; q++) {
+        sx += a.Lx[idx[q]];
+        sy += a.Ly[idx[q]];
+      }
+      lo[2] = sx;
+      lo[5] = sy;
+    }
+    {
+      const int32_t *off = a.tr_off[kTrSw], *idx = a.tr_idx[kTrSw];
+      double sx = 0.0, sy = 0.0;
+      for (int q = off[w]; q < off[w + 1]; q++) {
+        sx += a.Lx[idx[q]];
+        sy += a.Ly[idx[q]];
+      }
+      lo[3] = sx;
+      lo[7] = sy;
+    }
+    double ls[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) ls[k] = a.LS[k][w];
+    const int iee = a.ee[w], ine = a.ne[w], ise = a.se[w];
+    Corners c;
+    c.ucc = u[w];
+    c.vcc = v[w];
+    c.uee = u[iee];
+    c.vee = v[iee];
+    c.une = u[ine];
+    c.vne = v[ine];
+    c.use = u[ise];
+    c.vse = v[ise];
+    const Geom g = make_geom(a.dxT[w], a.dyT[w], a.HTE[w], a.HTN[w], a.HTEm1[w],
+                             a.HTNm1[w], p.deltaminEVP);
+    double lc[8], lstr;
+    stress_adjoint(c, g, a.strength[w], p, lo, ls, lc, lstr);
+#pragma unroll
+    for (int k = 0; k < 12; k++) a.LS[k][w] = ls[k];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a.C8[k][w] = lc[k];
+    a.g[kGStrength][w] += lstr;
+  }
+}
+
+// lam of the velocities at call start; fold_init adds the uvel_init part
+// when uvel_init was the call-start velocity.
+__global__ void __launch_bounds__(kThreads) k_adj_final(AdjArgs a, int fold_init) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.nslots;
+       x += gridDim.x * blockDim.x) {
+    double lu, lv;
+    velocity_lam(a, x, lu, lv);
+    if (fold_init) {
+      lu += a.g[kGUinit][x];
+      lv += a.g[kGVinit][x];
+    }
+    a.Pu[x] = lu;
+    a.Pv[x] = lv;
+  }
+}
+
+// Copy the halo slots [nslots, nslots+nhs) of src into entries 1..count-1 of
+// a tape whose entries are `stride` doubles apart.
+__global__ void k_fill_halo(double *tape, size_t stride, int nslots, int nhs, int count,
+                            const double *src) {
+  const long long total = (long long)nhs * (count - 1);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int e = 1 + (int)(t / nhs), j = (int)(t % nhs);
+    tape[(size_t)e * stride + nslots + j] = src[nslots + j];
+  }
+}
+
+int blocks_for(long long n) {
+  long long b = (n + kThreads - 1) / kThreads;
+  if (b < 1) b = 1;
+  if (b > 148LL * 64) b = 148LL * 64;
+  return (int)b;
+}
+
+// element counts rounded up to whole 256-byte lines
+size_t pad256(size_t doubles) { return (doubles + 31) & ~size_t(31); }
+size_t pad_ints(size_t n) { return (n + 63) & ~size_t(63); }
+
+}  // namespace
+
+struct AdjointState {
+  int device = 0;
+  // static part: transposed lists and work arrays (allocated once)
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
+  int32_t *tr_off[kNumTr] = {}, *tr_idx[kNumTr] = {};
+  double *Pu = nullptr, *Pv = nullptr, *Lx = nullptr, *Ly = nullptr;
+  double *C8[8] = {}, *LS[12] = {}, *g[kNumGrad] = {};
+  double *spp[2][12] = {};  // stress ping-pong of the segment recompute
+  // recording
+  void *store = nullptr;
+  size_t store_bytes = 0;
+  size_t stride = 0;    // doubles per velocity tape entry (nuv, padded)
+  size_t sstride = 0;   // doubles per stress array of a checkpoint (nslots, padded)
+  double *ck = nullptr;  // nseg checkpoints of u, v (stride each), 12 stresses
+  double *tape = nullptr;  // tape entries: u then v, 2*stride doubles each
+  bool valid = false, full_tape = false, uinit_explicit = false, seeded = false;
+  int ndte = 0, interval = 0, nseg = 0;
+  long long launches = 0;
+};
+
+void adjoint_release(AdjointState *a) {
+  if (!a) return;
+  cudaSetDevice(a->device);
+  if (a->store) cudaFree(a->store);
+  if (a->arena) cudaFree(a->arena);
+  delete a;
+}
+
+void adjoint_invalidate(AdjointState *a) {
+  if (a) {
+    a->valid = false;
+    a->seeded = false;
+  }
+}
+
+namespace {
+
+// Transposed neighbour lists and work arrays, built on first use.
+int ensure_static(evp1d_t *h) {
+  if (h->adj && h->adj->arena) return EVP1D_OK;
+  DeviceProblem &d = h->d;
+  if (!h->adj) h->adj = new AdjointState();
+  AdjointState &A = *h->adj;
+  A.device = d.device;
+  const int S = d.nslots;
+  cudaStream_t st = d.stream;
+  // neighbours and slot -> point map from the device
+  std::vector<int32_t> nb((size_t)6 * S), pos((size_t)S);
+  for (int k = 0; k < 6; k++)
+    ADJ_TRY(cudaMemcpyAsync(nb.data() + (size_t)k * S, d.nb[k], sizeof(int32_t) * S,
+                            cudaMemcpyDeviceToHost, st));
+  ADJ_TRY(cudaMemcpyAsync(pos.data(), d.point_of_slot, sizeof(int32_t) * S,
+                          cudaMemcpyDeviceToHost, st));
+  ADJ_TRY(cudaStreamSynchronize(st));
+  auto nbk = [&](int k, int s) { return nb[(size_t)k * S + s]; };
+  // (source neighbour vector, whether the edge is U->T or T->U) per list
+  // nb order: 0 ee, 1 ne, 2 se, 3 nw, 4 sw, 5 sse
+  const int src_nb[kNumTr] = {3, 5, 4, 0, 1, 2};
+  std::vector<std::vector<int32_t>> off(kNumTr), idx(kNumTr);
+  for (int t = 0; t < kNumTr; t++) {
+    std::vector<int32_t> cnt((size_t)S + 1, 0);
+    for (int s = 0; s < S; s++) {
+      if (pos[s] < 0) continue;
+      const int o = nbk(src_nb[t], s);
+      if (o >= 0 && o < S && pos[o] >= 0) cnt[o + 1]++;
+    }
+    for (int s = 0; s < S; s++) cnt[s + 1] += cnt[s];
+    off[t] = cnt;
+    idx[t].assign((size_t)cnt[S], 0);
+    std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
+    for (int s = 0; s < S; s++) {  // ascending s: a fixed summation order
+      if (pos[s] < 0) continue;
+      const int o = nbk(src_nb[t], s);
+      if (o >= 0 && o < S && pos[o] >= 0) idx[t][fill[o]++] = s;
+    }
+  }
+  // carve
+  const size_t SD = pad256((size_t)S);
+  size_t ints = 0;
+  for (int t = 0; t < kNumTr; t++) ints += pad_ints(off[t].size()) + pad_ints(idx[t].size() + 1);
+  const size_t ndbl = SD * (4 + 8 + 12 + kNumGrad + 24);
+  A.arena_bytes = ints * sizeof(int32_t) + ndbl * sizeof(double);
+  ADJ_TRY(cudaMalloc(&A.arena, A.arena_bytes));
+  double *pd = (double *)A.arena;
+  auto take = [&]() {
+    double *r = pd;
+    pd += SD;
+    return r;
+  };
+  A.Pu = take();
+  A.Pv = take();
+  A.Lx = take();
+  A.Ly = take();
+  for (int k = 0; k < 8; k++) A.C8[k] = take();
+  for (int k = 0; k < 12; k++) A.LS[k] = take();
+  for (int k = 0; k < kNumGrad; k++) A.g[k] = take();
+  for (int b = 0; b < 2; b++)
+    for (int k = 0; k < 12; k++) A.spp[b][k] = take();
+  int32_t *pi = (int32_t *)pd;
+  for (int t = 0; t < kNumTr; t++) {
+    A.tr_off[t] = pi;
+    pi += pad_ints(off[t].size());
+    A.tr_idx[t] = pi;
+    pi += pad_ints(idx[t].size() + 1);
+    ADJ_TRY(cudaMemcpyAsync(A.tr_off[t], off[t].data(), sizeof(int32_t) * off[t].size(),
+                            cudaMemcpyHostToDevice, st));
+    if (!idx[t].empty())
+      ADJ_TRY(cudaMemcpyAsync(A.tr_idx[t], idx[t].data(), sizeof(int32_t) * idx[t].size(),
+                              cudaMemcpyHostToDevice, st));
+  }
+  ADJ_TRY(cudaStreamSynchronize(st));  // the host vectors go out of scope
+  return EVP1D_OK;
+}
+
+AdjArgs adj_args(const evp1d_t *h) {
+  const DeviceProblem &d = h->d;
+  const AdjointState &A = *h->adj;
+  AdjArgs a;
+  a.nslots = d.nslots;
+  a.flags = d.flags;
+  a.ee = d.nb[0];
+  a.ne = d.nb[1];
+  a.se = d.nb[2];
+  for (int t = 0; t < kNumTr; t++) {
+    a.tr_off[t] = A.tr_off[t];
+    a.tr_idx[t] = A.tr_idx[t];
+  }
+  a.dxT = d.geo[kDxT];
+  a.dyT = d.geo[kDyT];
+  a.HTE = d.geo[kHTE];
+  a.HTN = d.geo[kHTN];
+  a.HTEm1 = d.geo[kHTEm1];
+  a.HTNm1 = d.geo[kHTNm1];
+  a.uarear = d.geo[kUarear];
+  a.strength = d.dyn[kStrength];
+  a.kvrel = d.dyn[kKvrel];
+  a.aiu = d.dyn[kAiu];
+  a.uocn = d.dyn[kUocn];
+  a.vocn = d.dyn[kVocn];
+  a.waterx = d.dyn[kWaterx];
+  a.watery = d.dyn[kWatery];
+  a.umassdti = d.dyn[kUmassdti];
+  a.fm = d.dyn[kFm];
+  a.Tbu = d.dyn[kTbu];
+  a.Pu = A.Pu;
+  a.Pv = A.Pv;
+  a.Lx = A.Lx;
+  a.Ly = A.Ly;
+  for (int k = 0; k < 8; k++) a.C8[k] = A.C8[k];
+  for (int k = 0; k < 12; k++) a.LS[k] = A.LS[k];
+  for (int k = 0; k < kNumGrad; k++) a.g[k] = A.g[k];
+  return a;
+}
+
+// One forward subcycle between explicit state buffers.
+void launch_state(evp1d_t *h, double *const s_in[12], double *const s_out[12],
+                  const double *u_in, const double *v_in, double *u_out, double *v_out,
+                  bool last) {
+  DeviceProblem &d = h->d;
+  if (h->path == kPathTma) {
+    TmaArgs a = problem_tma_args(d, 0);
+    a.prefetch = h->prefetch;
+    for (int k = 0; k < 12; k++) {
+      a.sf[7 + k] = s_in[k];
+      a.s_out[k] = s_out[k];
+    }
+    a.u_in = u_in;
+    a.v_in = v_in;
+    a.u_out = u_out;
+    a.v_out = v_out;
+    launch_tma(a, h->p, last, d.nctas, d.stream);
+  } else {
+    FusedArgs a = problem_fused_args(d, 0);
+    for (int k = 0; k < 12; k++) {
+      a.s_in[k] = s_in[k];
+      a.s_out[k] = s_out[k];
+    }
+    a.u_in = u_in;
+    a.v_in = v_in;
+    a.u_out = u_out;
+    a.v_out = v_out;
+    launch_fused(a, h->p, last, d.stream);
+  }
+}
+
+double *tape_u(AdjointState &A, int e) { return A.tape + (size_t)e * 2 * A.stride; }
+double *tape_v(AdjointState &A, int e) { return A.tape + (size_t)e * 2 * A.stride + A.stride; }
+double *ck_u(AdjointState &A, int j) {
+  return A.ck + (size_t)j * (2 * A.stride + 12 * A.sstride);
+}
+double *ck_v(AdjointState &A, int j) { return ck_u(A, j) + A.stride; }
+double *ck_s(AdjointState &A, int j, int k) {
+  return ck_u(A, j) + 2 * A.stride + (size_t)k * A.sstride;
+}
+
+int ensure_store(AdjointState &A, size_t bytes) {
+  if (A.store && A.store_bytes >= bytes) return EVP1D_OK;
+  if (A.store) cudaFree(A.store);
+  A.store = nullptr;
+  A.store_bytes = 0;
+  ADJ_TRY(cudaMalloc(&A.store, bytes));
+  A.store_bytes = bytes;
+  return EVP1D_OK;
+}
+
+}  // namespace
+}  // namespace evp
+
+using namespace evp;
+
+extern "C" {
+
+int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
+  if (!h) return error(EVP1D_ERR_INVALID_ARG, "NULL handle");
+  if (ndte < 1) return error(EVP1D_ERR_INVALID_ARG, "ndte = %d < 1", ndte);
+  if (!h->uploaded) return error(EVP1D_ERR_STATE, "evp1d_upload has not been called");
+  ADJ_TRY(cudaSetDevice(h->d.device));
+  DeviceProblem &d = h->d;
+  if (d.ntiles == 0) {  // nothing to differentiate
+    if (!h->adj) h->adj = new AdjointState();
+    h->adj->device = d.device;
+    h->adj->valid = true;
+    h->adj->ndte = ndte;
+    h->adj->nseg = 0;
+    h->adj->seeded = false;
+    return EVP1D_OK;
+  }
+  ADJ_CHECK(ensure_static(h));
+  AdjointState &A = *h->adj;
+  A.valid = false;
+  A.seeded = false;
+  A.stride = pad256((size_t)d.nuv);
+  A.sstride = pad256((size_t)d.nslots);
+  const size_t entry = 2 * A.stride * sizeof(double);
+  const size_t ckpt = (2 * A.stride + 12 * A.sstride) * sizeof(double);
+  bool full = false;
+  if (interval <= 0) {
+    size_t freeb = 0, totalb = 0;
+    ADJ_TRY(cudaMemGetInfo(&freeb, &totalb));
+    const size_t have = freeb + (A.store ? A.store_bytes : 0);
+    if ((size_t)(ndte + 1) * entry <= have / 2) {
+      full = true;
+    } else {
+      // fixed-interval checkpoints with the memory-minimising interval
+      // sqrt(ndte * checkpoint / tape entry)
+      interval = (int)std::ceil(std::sqrt((double)ndte * (double)ckpt / (double)entry));
+      interval = std::max(1, std::min(interval, ndte));
+    }
+  }
+  cudaStream_t st = d.stream;
+  const int cur0 = d.cur;
+  if (full) {
+    ADJ_CHECK(ensure_store(A, (size_t)(ndte + 1) * entry));
+    A.tape = (double *)A.store;
+    A.ck = nullptr;
+    A.full_tape = true;
+    A.interval = ndte;
+    A.nseg = 1;
+    ADJ_TRY(cudaMemcpyAsync(tape_u(A, 0), d.u[cur0], sizeof(double) * d.nuv,
+                            cudaMemcpyDeviceToDevice, st));
+    ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), d.v[cur0], sizeof(double) * d.nuv,
+                            cudaMemcpyDeviceToDevice, st));
+    if (d.nhs > 0) {
+      k_fill_halo<<<blocks_for((long long)d.nhs * ndte), kThreads, 0, st>>>(
+          A.tape, 2 * A.stride, d.nslots, d.nhs, ndte + 1, d.u[cur0]);
+      k_fill_halo<<<blocks_for((long long)d.nhs * ndte), kThreads, 0, st>>>(
+          A.tape + A.stride, 2 * A.stride, d.nslots, d.nhs, ndte + 1, d.v[cur0]);
+    }
+    int b = cur0;
+    for (int n = 0; n < ndte; n++) {
+      launch_state(h, d.stress[b], d.stress[1 - b], tape_u(A, n), tape_v(A, n),
+                   tape_u(A, n + 1), tape_v(A, n + 1), n == ndte - 1);
+      b = 1 - b;
+    }
+    h->launches += ndte;
+    // the final state back into the handle's buffers for evp1d_download
+    ADJ_TRY(cudaMemcpyAsync(d.u[b], tape_u(A, ndte), sizeof(double) * d.nslots,
+                            cudaMemcpyDeviceToDevice, st));
+    ADJ_TRY(cudaMemcpyAsync(d.v[b], tape_v(A, ndte), sizeof(double) * d.nslots,
+                            cudaMemcpyDeviceToDevice, st));
+    d.cur = b;
+  } else {
+    const int k = interval;
+    const int nseg = (ndte + k - 1) / k;
+    const size_t bytes = (size_t)nseg * ckpt + (size_t)(k + 1) * entry;
+    ADJ_CHECK(ensure_store(A, bytes));
+    A.ck = (double *)A.store;
+    A.tape = A.ck + (size_t)nseg * (ckpt / sizeof(double));
+    A.full_tape = false;
+    A.interval = k;
+    A.nseg = nseg;
+    // halo slots of the segment tape (entry 0 comes with each checkpoint)
+    if (d.nhs > 0 && k > 0) {
+      k_fill_halo<<<blocks_for((long long)d.nhs * k), kThreads, 0, st>>>(
+          A.tape, 2 * A.stride, d.nslots, d.nhs, k + 1, d.u[cur0]);
+      k_fill_halo<<<blocks_for((long long)d.nhs * k), kThreads, 0, st>>>(
+          A.tape + A.stride, 2 * A.stride, d.nslots, d.nhs, k + 1, d.v[cur0]);
+    }
+    for (int j = 0; j < nseg; j++) {
+      const int c = d.cur;
+      ADJ_TRY(cudaMemcpyAsync(ck_u(A, j), d.u[c], sizeof(double) * d.nuv,
+                              cudaMemcpyDeviceToDevice, st));
+      ADJ_TRY(cudaMemcpyAsync(ck_v(A, j), d.v[c], sizeof(double) * d.nuv,
+                              cudaMemcpyDeviceToDevice, st));
+      for (int q = 0; q < 12; q++)
+        ADJ_TRY(cudaMemcpyAsync(ck_s(A, j, q), d.stress[c][q], sizeof(double) * d.nslots,
+                                cudaMemcpyDeviceToDevice, st));
+      const int len = std::min(k, ndte - j * k);
+      ADJ_CHECK(evp1d_subcycles(h, len));
+    }
+  }
+  ADJ_TRY(cudaGetLastError());
+  A.ndte = ndte;
+  A.uinit_explicit = h->uinit_explicit;
+  A.valid = true;
+  return EVP1D_OK;
+}
+
+int evp1d_run_checkpointed(evp1d_t *h, int ndte, const evp1d_fields *io, int interval) {
+  ADJ_CHECK(evp1d_upload(h, io));
+  ADJ_CHECK(evp1d_record_subcycles(h, ndte, interval));
+  return evp1d_download(h, io);
+}
+
+int evp1d_adjoint_seed(evp1d_t *h, const double *lam_uvel, const double *lam_vvel,
+                       const double *const *lam_stress) {
+  if (!h) return error(EVP1D_ERR_INVALID_ARG, "NULL handle");
+  if (!h->adj || !h->adj->valid)
+    return error(EVP1D_ERR_STATE, "no recorded forward: call evp1d_run_checkpointed first");
+  DeviceProblem &d = h->d;
+  AdjointState &A = *h->adj;
+  if (d.ntiles == 0) {
+    A.seeded = true;
+    return EVP1D_OK;
+  }
+  if (!lam_uvel || !lam_vvel) return error(EVP1D_ERR_INVALID_ARG, "lam_uvel/lam_vvel are NULL");
+  ADJ_TRY(cudaSetDevice(d.device));
+  cudaStream_t st = d.stream;
+  const size_t nv = (size_t)(d.navel > 0 ? d.navel : 1);
+  const size_t bn = sizeof(double) * (size_t)d.na;
+  PermBatch b;
+  auto add = [&](const double *host, double *dst) -> int {
+    double *slot = d.stage + (size_t)b.n * nv;
+    ADJ_TRY(cudaMemcpyAsync(slot, host, bn, cudaMemcpyHostToDevice, st));
+    b.src[b.n] = slot;
+    b.dst[b.n] = dst;
+    b.n++;
+    return EVP1D_OK;
+  };
+  ADJ_CHECK(add(lam_uvel, A.Pu));
+  ADJ_CHECK(add(lam_vvel, A.Pv));
+  for (int k = 0; k < 12; k++) {
+    if (lam_stress && lam_stress[k])
+      ADJ_CHECK(add(lam_stress[k], A.LS[k]));
+    else
+      ADJ_TRY(cudaMemsetAsync(A.LS[k], 0, sizeof(double) * d.nslots, st));
+  }
+  launch_scatter(b, d.nslots, d.point_of_slot, st);
+  for (int k = 0; k < 8; k++)
+    ADJ_TRY(cudaMemsetAsync(A.C8[k], 0, sizeof(double) * d.nslots, st));
+  for (int k = 0; k < kNumGrad; k++)
+    ADJ_TRY(cudaMemsetAsync(A.g[k], 0, sizeof(double) * d.nslots, st));
+  ADJ_TRY(cudaGetLastError());
+  A.seeded = true;
+  return EVP1D_OK;
+}
+
+int evp1d_adjoint_sweep(evp1d_t *h) {
+  if (!h) return error(EVP1D_ERR_INVALID_ARG, "NULL handle");
+  if (!h->adj || !h->adj->valid)
+    return error(EVP1D_ERR_STATE, "no recorded forward: call evp1d_run_checkpointed first");
+  AdjointState &A = *h->adj;
+  if (!A.seeded) return error(EVP1D_ERR_STATE, "evp1d_adjoint_seed has not been called");
+  DeviceProblem &d = h->d;
+  A.seeded = false;  // the sweep consumes the seed
+  if (d.ntiles == 0) return EVP1D_OK;
+  ADJ_TRY(cudaSetDevice(d.device));
+  cudaStream_t st = d.stream;
+  const AdjArgs a = adj_args(h);
+  const int grid = blocks_for(d.nslots);
+  long long launches = 0;
+  auto reverse_step = [&](const double *u0, const double *v0, const double *u1,
+                          const double *v1) {
+    k_adj_stepu<<<grid, kThreads, 0, st>>>(a, h->p, u0, v0, u1, v1);
+    k_adj_stress<<<grid, kThreads, 0, st>>>(a, h->p, u0, v0);
+    launches += 2;
+  };
+  if (A.full_tape) {
+    for (int n = A.ndte - 1; n >= 0; n--)
+      reverse_step(tape_u(A, n), tape_v(A, n), tape_u(A, n + 1), tape_v(A, n + 1));
+  } else {
+    const int k = A.interval;
+    for (int j = A.nseg - 1; j >= 0; j--) {
+      const int len = std::min(k, A.ndte - j * k);
+      ADJ_TRY(cudaMemcpyAsync(tape_u(A, 0), ck_u(A, j), sizeof(double) * d.nuv,
+                              cudaMemcpyDeviceToDevice, st));
+      ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), ck_v(A, j), sizeof(double) * d.nuv,
+                              cudaMemcpyDeviceToDevice, st));
+      for (int q = 0; q < 12; q++)
+        ADJ_TRY(cudaMemcpyAsync(A.spp[0][q], ck_s(A, j, q), sizeof(double) * d.nslots,
+                                cudaMemcpyDeviceToDevice, st));
+      // recompute the segment's velocities from its checkpoint
+      for (int i = 0; i < len; i++) {
+        const int b = i & 1;
+        launch_state(h, A.spp[b], A.spp[1 - b], tape_u(A, i), tape_v(A, i),
+                     tape_u(A, i + 1), tape_v(A, i + 1), false);
+        launches++;
+      }
+      for (int i = len - 1; i >= 0; i--)
+        reverse_step(tape_u(A, i), tape_v(A, i), tape_u(A, i + 1), tape_v(A, i + 1));
+    }
+  }
+  k_adj_final<<<grid, kThreads, 0, st>>>(a, A.uinit_explicit ? 0 : 1);
+  launches++;
+  ADJ_TRY(cudaGetLastError());
+  A.launches = launches;
+  h->launches += launches;
+  return EVP1D_OK;
+}
+
+int evp1d_adjoint_gradients(evp1d_t *h, const evp1d_grads *g) {
+  if (!h || !g) return error(EVP1D_ERR_INVALID_ARG, "NULL argument");
+  if (!h->adj || !h->adj->valid)
+    return error(EVP1D_ERR_STATE, "no recorded forward: call evp1d_run_checkpointed first");
+  DeviceProblem &d = h->d;
+  AdjointState &A = *h->adj;
+  ADJ_TRY(cudaSetDevice(d.device));
+  cudaStream_t st = d.stream;
+  if (d.na == 0) return EVP1D_OK;
+  int code = 0;
+  ADJ_CHECK(problem_take_error(&d, &code));
+  if (code)
+    return error(EVP1D_ERR_TIMEOUT,
+                 "a bounded device wait ran out (code %d); the gradients are not valid", code);
+  const size_t nv = (size_t)(d.navel > 0 ? d.navel : 1);
+  const size_t bn = sizeof(double) * (size_t)d.na;
+  struct Out {
+    const double *src;
+    double *host;
+  };
+  std::vector<Out> outs;
+  auto want = [&](double *host, const double *src) {
+    if (host) outs.push_back({src, host});
+  };
+  want(g->strength, A.g[kGStrength]);
+  want(g->Cw, A.g[kGCw]);
+  want(g->forcex, A.g[kGForcex]);
+  want(g->forcey, A.g[kGForcey]);
+  want(g->uvel, A.Pu);
+  want(g->vvel, A.Pv);
+  for (int k = 0; k < 12; k++) want(g->stress[k], A.LS[k]);
+  if (A.uinit_explicit) {
+    want(g->uvel_init, A.g[kGUinit]);
+    want(g->vvel_init, A.g[kGVinit]);
+  } else {
+    if (g->uvel_init) memset(g->uvel_init, 0, bn);
+    if (g->vvel_init) memset(g->vvel_init, 0, bn);
+  }
+  for (size_t o = 0; o < outs.size(); o += kMaxBatch) {
+    PermBatch b;
+    for (size_t q = o; q < outs.size() && b.n < kMaxBatch; q++) {
+      b.src[b.n] = outs[q].src;
+      b.dst[b.n] = d.stage + (size_t)b.n * nv;
+      b.n++;
+    }
+    launch_gather(b, d.na, d.slot_of_point, st);
+    for (int q = 0; q < b.n; q++)
+      ADJ_TRY(cudaMemcpyAsync(outs[o + q].host, b.dst[q], bn, cudaMemcpyDeviceToHost, st));
+    ADJ_TRY(cudaStreamSynchronize(st));
+  }
+  ADJ_TRY(cudaGetLastError());
+  return EVP1D_OK;
+}
+
+int evp1d_adjoint(evp1d_t *h, const double *lam_uvel, const double *lam_vvel,
+                  const double *const *lam_stress, const evp1d_grads *g) {
+  ADJ_CHECK(evp1d_adjoint_seed(h, lam_uvel, lam_vvel, lam_stress));
+  ADJ_CHECK(evp1d_adjoint_sweep(h));
+  return evp1d_adjoint_gradients(h, g);
+}
+
+int evp1d_adjoint_info(evp1d_t *h, long long info[8]) {
+  if (!h || !info) return error(EVP1D_ERR_INVALID_ARG, "NULL argument");
+  for (int k = 0; k < 8; k++) info[k] = 0;
+  const AdjointState *A = h->adj;
+  if (!A) return EVP1D_OK;
+  info[0] = A->valid ? 1 : 0;
+  info[1] = A->full_tape ? 1 : 0;
+  info[2] = A->interval;
+  info[3] = A->nseg;
+  info[4] = (long long)A->store_bytes;
+  info[5] = (long long)A->arena_bytes;
+  info[6] = (long long)h->d.arena_bytes;
+  info[7] = A->launches;
+  return EVP1D_OK;
+}
+
+}  // extern "C"

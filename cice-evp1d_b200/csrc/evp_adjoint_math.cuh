@@ -1,0 +1,228 @@
+// evp_adjoint_math.cuh -- reverse-mode derivatives of one EVP subcycle at a
+// point (hand-written, FP64).
+//
+// The forward quantities a derivative needs are recomputed from the stored
+// velocities with the forward's own functions (evp_math.cuh), so every branch
+// takes the side the forward took: max(Delta, DminArea) (src/bench_v2b.F90:
+// 428-430), the capped/uncapped viscosity, and a zero-length square root
+// (Delta = 0, |u| = 0, |u_ocn - u| = 0), whose derivative is taken as 0.
+//
+// A "lam" value is the adjoint dJ/d(value) of a scalar loss J.  The stress
+// relaxation is linear in the old stresses with state-independent
+// coefficients, so the reverse sweep needs the velocities of each subcycle
+// but never the stresses.  These derivatives are not bit-matched to anything:
+// a reciprocal is multiplied where the forward divides.
+#pragma once
+
+#include "evp_math.cuh"
+
+namespace evp {
+
+// Transpose of str_combine (src/bench_v2b.F90:217-310): given lo[0..7] =
+// dJ/d str1..str8 at a point, add dJ/d s[0..11] (the updated stresses) to ls.
+__host__ __device__ __forceinline__ void str_combine_adjoint(const double (&lo)[8],
+                                                             const Geom &g,
+                                                             double (&ls)[12]) {
+  const double dxt = g.dxT, dyt = g.dyT, dxhy = g.dxhy, dyhx = g.dyhx;
+  // strp_tmp / strm_tmp of the four str pairs, and str12ew/we/ns/sn
+  const double l_pa = -lo[0] + lo[1], l_ma = -lo[0] + lo[1];
+  const double l_pb = -lo[2] + lo[3], l_mb = -lo[2] + lo[3];
+  const double l_pc = -lo[4] + lo[5], l_mc = lo[4] - lo[5];
+  const double l_pd = -lo[6] + lo[7], l_md = lo[6] - lo[7];
+  const double l_12ew = -lo[0] + lo[2], l_12we = -lo[1] + lo[3];
+  const double l_12ns = -lo[4] + lo[6], l_12sn = -lo[5] + lo[7];
+  // csig{p,m,12}{ne,nw,se,sw}
+  const double l_cpne = -dxhy * lo[0] - dyhx * lo[4], l_cmne = dxhy * lo[0] - dyhx * lo[4];
+  const double l_c12ne = dyhx * lo[0] + dxhy * lo[4];
+  const double l_cpnw = -dxhy * lo[1] - dyhx * lo[6], l_cmnw = dxhy * lo[1] - dyhx * lo[6];
+  const double l_c12nw = dyhx * lo[1] + dxhy * lo[6];
+  const double l_cpse = -dxhy * lo[2] - dyhx * lo[5], l_cmse = dxhy * lo[2] - dyhx * lo[5];
+  const double l_c12se = dyhx * lo[2] + dxhy * lo[5];
+  const double l_cpsw = -dxhy * lo[3] - dyhx * lo[7], l_cmsw = dxhy * lo[3] - dyhx * lo[7];
+  const double l_c12sw = dyhx * lo[3] + dxhy * lo[7];
+  const double ky3 = kP25 * dyt * kP333, ky6 = kP25 * dyt * kP166;
+  const double kx3 = kP25 * dxt * kP333, kx6 = kP25 * dxt * kP166;
+  const double hx3 = kP5 * dxt * kP333, hx6 = kP5 * dxt * kP166;
+  const double hy3 = kP5 * dyt * kP333, hy6 = kP5 * dyt * kP166;
+  // ssig{p,m,12}{n,s,e,w}
+  const double l_pn = ky3 * l_pa + ky6 * l_pb, l_ps = ky6 * l_pa + ky3 * l_pb;
+  const double l_pe = kx3 * l_pc + kx6 * l_pd, l_pw = kx6 * l_pc + kx3 * l_pd;
+  const double l_mn = ky3 * l_ma + ky6 * l_mb, l_ms = ky6 * l_ma + ky3 * l_mb;
+  const double l_me = kx3 * l_mc + kx6 * l_md, l_mw = kx6 * l_mc + kx3 * l_md;
+  const double l_12e = hx3 * l_12ew + hx6 * l_12we, l_12w = hx6 * l_12ew + hx3 * l_12we;
+  const double l_12n = hy3 * l_12ns + hy6 * l_12sn, l_12s = hy6 * l_12ns + hy3 * l_12sn;
+  // ssig{p,m,12}{1,2}
+  const double l_p1 = l_cpnw + l_cpse, l_p2 = l_cpne + l_cpsw;
+  const double l_m1 = l_cmnw + l_cmse, l_m2 = l_cmne + l_cmsw;
+  const double l_121 = l_c12nw + l_c12se, l_122 = l_c12ne + l_c12sw;
+  ls[0] += l_pn + l_pe + kP055 * l_p1 + kP111 * l_cpne + kP027 * l_cpsw;
+  ls[1] += l_pn + l_pw + kP055 * l_p2 + kP111 * l_cpnw + kP027 * l_cpse;
+  ls[2] += l_ps + l_pw + kP055 * l_p1 + kP111 * l_cpsw + kP027 * l_cpne;
+  ls[3] += l_ps + l_pe + kP055 * l_p2 + kP111 * l_cpse + kP027 * l_cpnw;
+  ls[4] += l_mn + l_me + kP055 * l_m1 + kP111 * l_cmne + kP027 * l_cmsw;
+  ls[5] += l_mn + l_mw + kP055 * l_m2 + kP111 * l_cmnw + kP027 * l_cmse;
+  ls[6] += l_ms + l_mw + kP055 * l_m1 + kP111 * l_cmsw + kP027 * l_cmne;
+  ls[7] += l_ms + l_me + kP055 * l_m2 + kP111 * l_cmse + kP027 * l_cmnw;
+  ls[8] += l_12n + l_12e + kP111 * l_121 + kP222 * l_c12ne + kP055 * l_c12sw;
+  ls[9] += l_12n + l_12w + kP111 * l_122 + kP222 * l_c12nw + kP055 * l_c12se;
+  ls[10] += l_12s + l_12w + kP111 * l_121 + kP222 * l_c12sw + kP055 * l_c12ne;
+  ls[11] += l_12s + l_12e + kP111 * l_122 + kP222 * l_c12se + kP055 * l_c12nw;
+}
+
+// Reverse of one corner's relaxation (corner_update with visc_replpress,
+// src/bench_v2b.F90:186-212, 415-437).  In: l_sp, l_sm, l_s12 = lam of the
+// updated stresses of the corner.  Out: lam of the old stresses (returned in
+// place), lam of the corner's div, ten, shr (through Delta as well) and the
+// corner's contribution to dJ/dstrength.
+__host__ __device__ __forceinline__ void corner_adjoint(
+    double &l_sp, double &l_sm, double &l_s12, double div, double ten, double shr,
+    double Delta, double strength, double DminArea, const Params &p, double &l_div,
+    double &l_ten, double &l_shr, double &l_strength) {
+  const double a = p.arlx1i, d = p.denom1;
+  const double keep = (kC1 - a * p.revp) * d;
+  const double A = l_sp * d * a;          // lam of (zetax2*div - rep_prs)
+  const double B = l_sm * d * a;          // lam of etax2*ten
+  const double Cc = l_s12 * d * a * kP5;  // lam of etax2*shr
+  l_sp *= keep;
+  l_sm *= keep;
+  l_s12 *= keep;
+  // the forward's viscosity (tmpcalc) and its derivatives
+  const bool above = Delta > DminArea;  // max(Delta, DminArea) picked Delta
+  const double inv_m = kC1 / (above ? Delta : DminArea);
+  double tmp, dtmp_dstr, dtmp_dD;
+  if (p.capping == kC1) {
+    tmp = strength * inv_m;
+    dtmp_dstr = inv_m;
+    dtmp_dD = above ? -tmp * inv_m : 0.0;
+  } else {
+    const double inv_p = kC1 / (Delta + DminArea);
+    tmp = p.capping * (strength * inv_m) + (kC1 - p.capping) * (strength * inv_p);
+    dtmp_dstr = p.capping * inv_m + (kC1 - p.capping) * inv_p;
+    dtmp_dD = (above ? -p.capping * strength * inv_m * inv_m : 0.0) -
+              (kC1 - p.capping) * strength * inv_p * inv_p;
+  }
+  const double z = (kC1 + p.Ktens) * tmp, e = p.epp2i * z;
+  // zetax2 = (1+Ktens)*tmp, etax2 = epp2i*zetax2, rep_prs = (1-Ktens)*tmp*Delta
+  const double l_e = B * ten + Cc * shr;
+  const double l_z = A * div + p.epp2i * l_e;
+  const double l_r = -A;
+  const double l_tmp = (kC1 + p.Ktens) * l_z + (kC1 - p.Ktens) * Delta * l_r;
+  const double l_Delta = (kC1 - p.Ktens) * tmp * l_r + l_tmp * dtmp_dD;
+  l_strength = l_tmp * dtmp_dstr;
+  l_div = A * z;
+  l_ten = B * e;
+  l_shr = Cc * e;
+  // Delta = sqrt(div^2 + e_factor*(ten^2 + shr^2))
+  if (Delta > 0.0) {
+    const double q = l_Delta * (above ? inv_m : kC1 / Delta);
+    l_div += q * div;
+    l_ten += q * p.e_factor * ten;
+    l_shr += q * p.e_factor * shr;
+  }
+}
+
+// Transpose of strain_rates (src/bench_v2b.F90:363-395): lam of the corner
+// velocities from lam of div, ten, shr at the corners ne, nw, sw, se.
+// out[0..7] = lam of ucc, vcc, uee, vee, une, vne, use, vse.
+__host__ __device__ __forceinline__ void strain_adjoint(const double (&D)[4],
+                                                        const double (&T)[4],
+                                                        const double (&H)[4],
+                                                        const Geom &g, double (&out)[8]) {
+  const double dxT = g.dxT, dyT = g.dyT, cxp = g.cxp, cyp = g.cyp, cxm = g.cxm, cym = g.cym;
+  out[0] = cyp * D[0] + dyT * D[1] - cym * T[0] + dyT * T[1] - cxm * H[0] + dxT * H[3];
+  out[1] = cxp * D[0] + dxT * D[3] + cxm * T[0] - dxT * T[3] - cym * H[0] + dyT * H[1];
+  out[2] = -dyT * D[0] + cym * D[1] - dyT * T[0] - cyp * T[1] - cxm * H[1] + dxT * H[2];
+  out[3] = cxp * D[1] + dxT * D[2] + cxm * T[1] - dxT * T[2] - dyT * H[0] - cyp * H[1];
+  out[4] = cym * D[2] - dyT * D[3] - cyp * T[2] - dyT * T[3] - dxT * H[1] - cxp * H[2];
+  out[5] = -dxT * D[1] + cxm * D[2] + dxT * T[1] + cxp * T[2] - cyp * H[2] - dyT * H[3];
+  out[6] = dyT * D[2] + cyp * D[3] + dyT * T[2] - cym * T[3] - dxT * H[0] - cxp * H[3];
+  out[7] = -dxT * D[0] + cxm * D[3] + dxT * T[0] + cxp * T[3] + dyT * H[2] - cym * H[3];
+}
+
+// Reverse of stress at one T point.  lo = lam of str1..str8 written by the
+// subcycle, ls = lam of the updated stresses (in: from later subcycles; out:
+// lam of the old stresses).  Returns the lam of the 8 corner velocities and
+// the point's dJ/dstrength contribution.
+__host__ __device__ __forceinline__ void stress_adjoint(const Corners &c, const Geom &g,
+                                                        double strength, const Params &p,
+                                                        const double (&lo)[8],
+                                                        double (&ls)[12], double (&lc)[8],
+                                                        double &l_strength) {
+  str_combine_adjoint(lo, g, ls);
+  const Strain sr = strain_rates(c, g, p.e_factor);
+  double D[4], T[4], H[4];
+  l_strength = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    double lst;
+    corner_adjoint(ls[k], ls[4 + k], ls[8 + k], sr.div[k], sr.ten[k], sr.shr[k],
+                   sr.Delta[k], strength, g.DminTarea, p, D[k], T[k], H[k], lst);
+    l_strength += lst;
+  }
+  strain_adjoint(D, T, H, g, lc);
+}
+
+// Reverse of stepu at one U point (src/bench_v2b.F90:509-544) from the
+// velocity before (uold, vold) and after (unew, vnew) the subcycle.  cc1 and
+// cc2 are recovered from the solved velocity, [cc1; cc2] = [[cca, -ccb],
+// [ccb, cca]] [unew; vnew].
+struct StepuAdjIn {
+  double uold, vold, unew, vnew;
+  double lun, lvn;  // lam of unew, vnew
+  double kvrel, aiXrhow, uocn, vocn, waterx, watery, umassdti, fm, Tbu;
+};
+struct StepuAdjOut {
+  double luold, lvold;  // lam of uold, vold through this stepu
+  double lcc1, lcc2;    // lam of strintx + forcex + ..., i.e. of strintx, forcex
+  double gCw;           // dJ/dCw contribution
+  double luinit, lvinit;
+};
+
+__host__ __device__ __forceinline__ StepuAdjOut stepu_adjoint(const StepuAdjIn &in,
+                                                              const Params &p) {
+  StepuAdjOut o;
+  const double u = in.uold, v = in.vold;
+  const double du = in.uocn - u, dv = in.vocn - v;
+  const double sq = sqrt(du * du + dv * dv);
+  const double vrel = in.kvrel * sq;
+  const double sn = sqrt(u * u + v * v);
+  const double den = sn + p.u0;
+  const double Cb = in.Tbu / den;
+  const double cca = (p.brlx + p.revp) * in.umassdti + vrel * p.cosw + Cb;
+  const double sg = copysign(kC1, in.fm);
+  const double ccb = in.fm + sg * vrel * p.sinw;
+  const double inv_ab2 = kC1 / (cca * cca + ccb * ccb);
+  const double cc1 = cca * in.unew - ccb * in.vnew;
+  const double cc2 = ccb * in.unew + cca * in.vnew;
+  // unew = (cca*cc1 + ccb*cc2)/ab2, vnew = (cca*cc2 - ccb*cc1)/ab2
+  const double lN1 = in.lun * inv_ab2, lN2 = in.lvn * inv_ab2;
+  const double lab2 = -(in.lun * in.unew + in.lvn * in.vnew) * inv_ab2;
+  const double lcca = lN1 * cc1 + lN2 * cc2 + lab2 * 2.0 * cca;
+  const double lccb = lN1 * cc2 - lN2 * cc1 + lab2 * 2.0 * ccb;
+  o.lcc1 = lN1 * cca - lN2 * ccb;
+  o.lcc2 = lN1 * ccb + lN2 * cca;
+  // cc1 = strintx + forcex + vrel*waterx + umassdti*(brlx*u + revp*uinit)
+  double lu = o.lcc1 * in.umassdti * p.brlx, lv = o.lcc2 * in.umassdti * p.brlx;
+  o.luinit = o.lcc1 * in.umassdti * p.revp;
+  o.lvinit = o.lcc2 * in.umassdti * p.revp;
+  const double lvrel = o.lcc1 * in.waterx + o.lcc2 * in.watery + lcca * p.cosw +
+                       lccb * sg * p.sinw;
+  // Cb = Tbu/(sqrt(u^2+v^2) + u0)
+  if (in.Tbu != 0.0 && sn > 0.0) {
+    const double lsn = -lcca * Cb / (den * sn);
+    lu += lsn * u;
+    lv += lsn * v;
+  }
+  // vrel = (aiX*rhow*Cw) * sqrt(du^2 + dv^2)
+  o.gCw = lvrel * sq * in.aiXrhow;
+  if (sq > 0.0) {
+    const double lsq = lvrel * in.kvrel / sq;
+    lu -= lsq * du;
+    lv -= lsq * dv;
+  }
+  o.luold = lu;
+  o.lvold = lv;
+  return o;
+}
+
+}  // namespace evp

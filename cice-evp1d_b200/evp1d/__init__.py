@@ -244,6 +244,70 @@ class EVP1D:
     def stepu_only(self, n: int) -> None:
         check(self._L.evp1d_stepu_only(self.h, int(n)), "evp1d_stepu_only")
 
+    # -- adjoint ----------------------------------------------------------
+    GRADS = ("strength", "Cw", "forcex", "forcey", "uvel", "vvel")
+
+    def run_checkpointed(self, ndte: int, fields: FieldSet, interval: int = 0) -> FieldSet:
+        """evp1d_run that also records what :meth:`adjoint` needs (interval > 0:
+        checkpoints every `interval` subcycles; 0: sized to device memory)."""
+        check(self._L.evp1d_run_checkpointed(self.h, int(ndte), C.byref(fields.c),
+                                             int(interval)), "evp1d_run_checkpointed")
+        return fields
+
+    def record_subcycles(self, ndte: int, interval: int = 0) -> None:
+        check(self._L.evp1d_record_subcycles(self.h, int(ndte), int(interval)),
+              "evp1d_record_subcycles")
+
+    def _lam_stress(self, lam_stress):
+        if lam_stress is None:
+            return None, None
+        ls = np.ascontiguousarray(lam_stress, dtype=np.float64)
+        if ls.shape != (12, self.na):
+            raise ValueError(f"lam_stress: expected (12, {self.na})")
+        arr = (_D * 12)(*[ls[k].ctypes.data_as(_D) for k in range(12)])
+        return ls, arr
+
+    def adjoint_seed(self, lam_u, lam_v, lam_stress=None) -> None:
+        lu = _as_f64(lam_u, self.na, "lam_u")
+        lv = _as_f64(lam_v, self.na, "lam_v")
+        keep, arr = self._lam_stress(lam_stress)
+        check(self._L.evp1d_adjoint_seed(self.h, _d(lu), _d(lv), arr), "evp1d_adjoint_seed")
+
+    def adjoint_sweep(self) -> None:
+        check(self._L.evp1d_adjoint_sweep(self.h), "evp1d_adjoint_sweep")
+
+    def adjoint_gradients(self, want=GRADS, stress: bool = False,
+                          init: bool = False) -> dict:
+        out = {k: np.zeros(self.na) for k in want}
+        g = _lib.Grads()
+        for k, a in out.items():
+            setattr(g, k, _d(a))
+        if stress:
+            out["stress"] = np.zeros((12, self.na))
+            for k in range(12):
+                g.stress[k] = out["stress"][k].ctypes.data_as(_D)
+        if init:
+            out["uvel_init"] = np.zeros(self.na)
+            out["vvel_init"] = np.zeros(self.na)
+            g.uvel_init, g.vvel_init = _d(out["uvel_init"]), _d(out["vvel_init"])
+        check(self._L.evp1d_adjoint_gradients(self.h, C.byref(g)), "evp1d_adjoint_gradients")
+        return out
+
+    def adjoint(self, lam_u, lam_v, lam_stress=None, want=GRADS, stress: bool = False,
+                init: bool = False) -> dict:
+        """Gradients of J from dJ/d(final uvel, vvel) [na] (and optionally
+        dJ/d(final stresses) [12, na]) for the last recorded forward."""
+        self.adjoint_seed(lam_u, lam_v, lam_stress)
+        self.adjoint_sweep()
+        return self.adjoint_gradients(want, stress=stress, init=init)
+
+    def adjoint_info(self) -> dict:
+        info = (C.c_longlong * 8)()
+        check(self._L.evp1d_adjoint_info(self.h, info), "evp1d_adjoint_info")
+        keys = ("valid", "full_tape", "interval", "segments", "store_bytes",
+                "work_bytes", "solver_bytes", "sweep_launches")
+        return {k: int(v) for k, v in zip(keys, info)}
+
     def set_params(self, params: Params) -> None:
         check(self._L.evp1d_set_params(self.h, C.byref(params)), "evp1d_set_params")
         self.params = params

@@ -46,6 +46,15 @@ class Fields(C.Structure):
     ]
 
 
+class Grads(C.Structure):
+    """evp1d_grads (include/evp1d.h)."""
+    _fields_ = [
+        ("strength", _D), ("Cw", _D), ("forcex", _D), ("forcey", _D),
+        ("uvel", _D), ("vvel", _D), ("stress", _D * 12),
+        ("uvel_init", _D), ("vvel_init", _D),
+    ]
+
+
 class EVP1DError(RuntimeError):
     def __init__(self, code: int, where: str, msg: str):
         super().__init__(f"{where}: {ERRORS.get(code, code)}: {msg}")
@@ -99,6 +108,17 @@ def load() -> C.CDLL:
                                      C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)] + [_I] * 9)
     L.evp1d_plan_stats.argtypes = [C.c_int, C.c_int] + [_I] * 6 + [C.POINTER(C.c_longlong)]
+    L.evp1d_run_checkpointed.argtypes = [H, C.c_int, C.POINTER(Fields), C.c_int]
+    L.evp1d_record_subcycles.argtypes = [H, C.c_int, C.c_int]
+    L.evp1d_adjoint.argtypes = [H, _D, _D, C.POINTER(_D), C.POINTER(Grads)]
+    L.evp1d_adjoint_seed.argtypes = [H, _D, _D, C.POINTER(_D)]
+    L.evp1d_adjoint_sweep.argtypes = [H]
+    L.evp1d_adjoint_gradients.argtypes = [H, C.POINTER(Grads)]
+    L.evp1d_adjoint_info.argtypes = [H, C.POINTER(C.c_longlong)]
+    for name in ("evp1d_run_checkpointed", "evp1d_record_subcycles", "evp1d_adjoint",
+                 "evp1d_adjoint_seed", "evp1d_adjoint_sweep", "evp1d_adjoint_gradients",
+                 "evp1d_adjoint_info"):
+        getattr(L, name).restype = C.c_int
     L.evp1d_run_device_noalloc.argtypes = ([C.c_int, C.c_int] + [C.c_void_p] * 13
                                            + [C.POINTER(Params), C.c_int,
                                               C.POINTER(Fields), C.c_void_p])

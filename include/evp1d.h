@@ -246,6 +246,59 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
                      const int32_t *sse, long long stats[8]);
 
 /* ----------------------------------------------------------------------------
+ * Adjoint (reverse-mode gradients) of the subcycle loop.  No counterpart in
+ * the reference, whose loop is forward only.
+ *
+ * 1. evp1d_run_checkpointed: the same call as evp1d_run, recording what the
+ *    reverse sweep needs on the device:
+ *      interval > 0:  (u, v, 12 stresses) every `interval` subcycles; the
+ *                     sweep recomputes each segment's velocities from its
+ *                     checkpoint (one extra forward in all);
+ *      interval <= 0: sized to device memory: every subcycle's velocities
+ *                     when they fit in half of the free memory (no
+ *                     recompute), else checkpoints at the interval
+ *                     ceil(sqrt(ndte * checkpoint size / velocity size)),
+ *                     which minimises memory.
+ * 2. evp1d_adjoint: given dJ/d uvel, dJ/d vvel of the call's final list-point
+ *    velocities ([na], host) and optionally dJ/d of the final stresses
+ *    (lam_stress: NULL, or 12 pointers of which any may be NULL), writes the
+ *    requested gradients ([na] host arrays; NULL = not wanted):
+ *      strength, Cw (per point; for a scalar Cw sum them), forcex, forcey,
+ *      uvel, vvel, stress[12] (with respect to the call's starting values),
+ *      uvel_init, vvel_init (only when the recorded call passed them; when
+ *      it did not, their gradient is part of uvel, vvel and these are 0).
+ * Derivatives take the branch the forward took at max(Delta, DminArea) and
+ * are 0 at a zero-length square root.  The recorded forward is dropped by the
+ * next evp1d_upload or evp1d_set_params; one recording can be swept any
+ * number of times with different seeds.  Works on batched handles (gradients
+ * per member in the member-major [na] layout).
+ * -------------------------------------------------------------------------- */
+typedef struct evp1d_grads {
+  double *strength, *Cw, *forcex, *forcey;
+  double *uvel, *vvel;
+  double *stress[12];
+  double *uvel_init, *vvel_init;
+} evp1d_grads;
+
+int evp1d_run_checkpointed(evp1d_t *handle, int ndte, const evp1d_fields *io,
+                           int interval);
+int evp1d_adjoint(evp1d_t *handle, const double *lam_uvel, const double *lam_vvel,
+                  const double *const *lam_stress, const evp1d_grads *grads);
+/* The same two calls split for device-resident timing: the recording forward
+ * after evp1d_upload; the seed upload, the reverse sweep (queued on the
+ * handle's stream) and the gradient download. */
+int evp1d_record_subcycles(evp1d_t *handle, int ndte, int interval);
+int evp1d_adjoint_seed(evp1d_t *handle, const double *lam_uvel, const double *lam_vvel,
+                       const double *const *lam_stress);
+int evp1d_adjoint_sweep(evp1d_t *handle);
+int evp1d_adjoint_gradients(evp1d_t *handle, const evp1d_grads *grads);
+/* info[0] 1 if a recorded forward is held, [1] 1 for a full velocity tape,
+ * [2] checkpoint interval, [3] segments, [4] bytes of checkpoints and tape,
+ * [5] bytes of the adjoint work arrays, [6] bytes of the forward solver,
+ * [7] kernel launches of the last sweep. */
+int evp1d_adjoint_info(evp1d_t *handle, long long info[8]);
+
+/* ----------------------------------------------------------------------------
  * Allocation-free entry point.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory -- device memory owned by

@@ -1,0 +1,202 @@
+"""GPU tests of the adjoint (evp1d_run_checkpointed + evp1d_adjoint) through
+the C-ABI, against the taped FP64 torch restatement (oracle/evp_tape.py) and
+central finite differences of the bit-exact GPU forward.
+
+Tolerances: gradients agree with the tape to 1e-9 relative (max-norm over
+the field; the two differ only by rounding order); directional derivatives
+agree with central differences (step 1e-6 relative) to 1e-6 relative;
+checkpointed and full-tape sweeps agree bit for bit; an ensemble member's
+gradients agree with the member solved alone to 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+import evp1d
+from evp1d import synth
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("strength", "Cw", "forcex", "forcey")
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def small(seed=41, nx=60, ny=45, ndte=15, curvilinear=True):
+    return synth.to_1d(synth.make_grid(nx, ny, seed=seed, ndte=ndte, curvilinear=curvilinear))
+
+
+def gpu_grads(pr, ndte, uobs, vobs, interval=0, stress=False, lam_stress=None):
+    fs = evp1d.FieldSet.from_problem(pr)
+    with evp1d.EVP1D.from_problem(pr, ndte=ndte) as s:
+        s.run_checkpointed(ndte, fs, interval)
+        na = pr.na
+        lu = 2.0 * (fs.uvel[:na] - uobs)
+        lv = 2.0 * (fs.vvel[:na] - vobs)
+        g = s.adjoint(lu, lv, lam_stress=lam_stress, stress=stress)
+        info = s.adjoint_info()
+    return g, fs, info
+
+
+@pytest.mark.parametrize("curvilinear", [False, True])
+@pytest.mark.parametrize("interval", [0, 4, 15, 40])
+def test_adjoint_matches_tape(oracle_mod, curvilinear, interval):
+    import evp_tape
+    pr = small(curvilinear=curvilinear)
+    ndte = pr.ndte
+    uobs, vobs = synth.observations(pr.na, seed=77)
+    p = evp1d.set_evp_parameters(ndte)
+    g, fs, info = gpu_grads(pr, ndte, uobs, vobs, interval=interval, stress=True)
+    assert info["valid"] == 1
+    assert info["full_tape"] == (1 if interval == 0 else 0)
+    t = evp_tape.gradient(pr, ndte, p, uobs, vobs)
+    for k in FIELDS:
+        assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
+    assert rel(g["uvel"], t["uvel0"]) < 1e-9
+    assert rel(g["vvel"], t["vvel0"]) < 1e-9
+    assert rel(g["stress"], t["stress0"]) < 1e-9
+
+
+def test_checkpointed_forward_is_the_forward(oracle_mod):
+    """run_checkpointed returns exactly evp1d_run's outputs, in both modes."""
+    pr = small(seed=43, ndte=23)
+    ref = evp1d.FieldSet.from_problem(pr, want_str=True)
+    with evp1d.EVP1D.from_problem(pr) as s:
+        s.run(pr.ndte, ref)
+    for interval in (0, 5, 50):
+        fs = evp1d.FieldSet.from_problem(pr, want_str=True)
+        with evp1d.EVP1D.from_problem(pr) as s:
+            s.run_checkpointed(pr.ndte, fs, interval)
+        for a, b in ((fs.stress, ref.stress), (fs.uvel, ref.uvel), (fs.vvel, ref.vvel),
+                     (fs.strintx, ref.strintx), (fs.strinty, ref.strinty), (fs.Cb, ref.Cb),
+                     (fs.str, ref.str)):
+            assert np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+def test_checkpoint_and_tape_sweeps_agree_bitwise():
+    pr = small(seed=45, ndte=31)
+    uobs, vobs = synth.observations(pr.na, seed=3)
+    ga, _, ia = gpu_grads(pr, pr.ndte, uobs, vobs, interval=0)
+    for interval in (1, 7, 31, 100):
+        gb, _, ib = gpu_grads(pr, pr.ndte, uobs, vobs, interval=interval)
+        assert ib["segments"] == -(-pr.ndte // min(interval, 100))
+        for k in ga:
+            assert np.array_equal(ga[k].view(np.int64), gb[k].view(np.int64)), (interval, k)
+
+
+def central_difference(run, pr, field, d, h, uobs, vobs):
+    """(J(p + h d) - J(p - h d)) / 2h for J = sum (u-u_obs)^2 + (v-v_obs)^2,
+    summed point by point as (u+ - u-)(u+ + u- - 2 u_obs) so that the
+    difference does not cancel against the size of J."""
+    prp, prm = pr.copy(), pr.copy()
+    prp.f[field] = pr.f[field] + h * d
+    prm.f[field] = pr.f[field] - h * d
+    up, vp = run(prp)
+    um, vm = run(prm)
+    return float(np.sum((up - um) * (up + um - 2 * uobs) + (vp - vm) * (vp + vm - 2 * vobs))) / (2 * h)
+
+
+def test_adjoint_matches_finite_differences():
+    """cfg1-sized grid (400 x 300), ndte = 120: directional derivatives of J
+    along 8 random directions per field against central differences of the
+    GPU forward, step 1e-6 relative."""
+    pr = synth.make_problem("cfg1")
+    ndte = pr.ndte
+    uobs, vobs = synth.observations(pr.na, seed=404)
+    g, fs0, _ = gpu_grads(pr, ndte, uobs, vobs, interval=synth.ADJOINT_INTERVAL)
+    na = pr.na
+    rng = np.random.default_rng(8)
+    h = 1e-6
+    with evp1d.EVP1D.from_problem(pr, ndte=ndte) as s:
+        def run(prx):
+            fs = evp1d.FieldSet.from_problem(prx)
+            s.run(ndte, fs)
+            return fs.uvel[:na].copy(), fs.vvel[:na].copy()
+        worst = {}
+        for k in FIELDS:
+            for _ in range(8):
+                d = pr.f[k] * rng.standard_normal(na)
+                fd = central_difference(run, pr, k, d, h, uobs, vobs)
+                ad = float(np.dot(g[k], d))
+                err = abs(fd - ad) / max(abs(ad), 1e-300)
+                worst[k] = max(worst.get(k, 0.0), err)
+                assert err <= 1e-6, (k, fd, ad)
+    print("worst FD relative error per field", {k: f"{v:.1e}" for k, v in worst.items()})
+
+
+def test_adjoint_is_linear_in_the_seed_and_reusable():
+    pr = small(seed=47, ndte=12)
+    fs = evp1d.FieldSet.from_problem(pr)
+    rng = np.random.default_rng(1)
+    a = rng.normal(size=(2, pr.na))
+    b = rng.normal(size=(2, pr.na))
+    with evp1d.EVP1D.from_problem(pr) as s:
+        s.run_checkpointed(pr.ndte, fs, 5)
+        ga = s.adjoint(a[0], a[1])
+        gb = s.adjoint(b[0], b[1])
+        gab = s.adjoint(a[0] + b[0], a[1] + b[1])
+        ga2 = s.adjoint(a[0], a[1])
+    for k in ga:
+        assert rel(gab[k], ga[k] + gb[k]) < 1e-12, k
+        assert np.array_equal(ga[k], ga2[k]), k
+
+
+def test_adjoint_explicit_uvel_init(oracle_mod):
+    """With uvel_init given, its gradient is reported apart (revp = 1 makes
+    it nonzero) and matches the tape."""
+    import evp_tape
+    pr = small(seed=49, ndte=9)
+    p = evp1d.set_evp_parameters(pr.ndte)
+    p.revp = 1.0
+    uobs, vobs = synth.observations(pr.na, seed=5)
+    fs = evp1d.FieldSet.from_problem(pr, explicit_init=True)
+    with evp1d.EVP1D.from_problem(pr, params=p) as s:
+        s.run_checkpointed(pr.ndte, fs, 0)
+        g = s.adjoint(2 * (fs.uvel[: pr.na] - uobs), 2 * (fs.vvel[: pr.na] - vobs), init=True)
+    t = evp_tape.gradient(pr, pr.ndte, p, uobs, vobs,
+                          wrt=("forcex", "uvel0", "vvel0", "uvel_init", "vvel_init"))
+    assert np.abs(g["uvel_init"]).max() > 0
+    assert rel(g["uvel_init"], t["uvel_init"]) < 1e-9
+    assert rel(g["vvel_init"], t["vvel_init"]) < 1e-9
+    assert rel(g["uvel"], t["uvel0"]) < 1e-9
+    assert rel(g["forcex"], t["forcex"]) < 1e-9
+
+
+def test_batched_adjoint_matches_members():
+    members = [small(seed=51 + m, nx=30 + 17 * m, ny=28, ndte=20) for m in range(3)]
+    ens = synth.concat(members)
+    ndte = 20
+    obs = [synth.observations(m.na, seed=600 + i) for i, m in enumerate(members)]
+    uobs = np.concatenate([o[0] for o in obs])
+    vobs = np.concatenate([o[1] for o in obs])
+    fs = evp1d.FieldSet.from_problem(ens.combined)
+    with evp1d.EVP1D.batched(ens, ndte=ndte) as s:
+        s.run_checkpointed(ndte, fs, 0)
+        # list-point velocities of the member-major layout
+        u_list = np.concatenate([u[: m.na] for u, m in zip(ens.split_slots(fs.uvel), members)])
+        v_list = np.concatenate([v[: m.na] for v, m in zip(ens.split_slots(fs.vvel), members)])
+        g = s.adjoint(2 * (u_list - uobs), 2 * (v_list - vobs))
+    off = 0
+    for i, m in enumerate(members):
+        gm, _, _ = gpu_grads(m, ndte, obs[i][0], obs[i][1], interval=0)
+        for k in FIELDS:
+            assert rel(g[k][off: off + m.na], gm[k]) <= 1e-10, (i, k)
+        off += m.na
+
+
+def test_adjoint_state_errors():
+    pr = small(seed=53, ndte=4)
+    fs = evp1d.FieldSet.from_problem(pr)
+    z = np.zeros(pr.na)
+    with evp1d.EVP1D.from_problem(pr) as s:
+        with pytest.raises(evp1d.EVP1DError) as e:
+            s.adjoint(z, z)
+        assert e.value.code == -7
+        s.run_checkpointed(pr.ndte, fs, 2)
+        s.adjoint(z, z)
+        s.upload(fs)  # new inputs drop the recording
+        with pytest.raises(evp1d.EVP1DError) as e:
+            s.adjoint(z, z)
+        assert e.value.code == -7
