@@ -287,6 +287,258 @@ def run_ensemble(args, rank, world, local):
 
 
 # --------------------------------------------------------------------------
+# GPU: adjoint configurations
+# --------------------------------------------------------------------------
+ADJ_METRIC = "EVP adjoint ice-point-subcycles/s (FP64)"
+
+
+def _misfit_seed(u, v, uobs, vobs):
+    return 2.0 * (u - uobs), 2.0 * (v - vobs)
+
+
+def _timed(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1000.0
+
+
+def _adjoint_once(s, stream, ndte, interval, lam, fields):
+    """One gradient from the initial state: upload (untimed), the recording
+    forward, then seed + reverse sweep, each timed with CUDA events on the
+    solver's stream."""
+    s.upload(fields())
+    t_rec = _timed(stream, lambda: s.record_subcycles(ndte, interval))
+    s.adjoint_seed(*lam)
+    t_sw = _timed(stream, s.adjoint_sweep)
+    s.synchronize()
+    return t_rec, t_sw
+
+
+def run_adjoint(args, rank, world, local):
+    """Single-problem adjoint (800 x 600, ndte = 500, J = misfit of the final
+    velocities, checkpoints every 50 subcycles): forward, recording forward and
+    reverse sweep timed on the device; a finite-difference check along 32
+    random directions (8 per gradient field)."""
+    import numpy as np
+    import torch
+    import evp1d
+    from evp1d import synth
+
+    torch.cuda.set_device(local)
+    over = {"ndte": args.ndte} if args.ndte else {}
+    seed = synth.CONFIGS[args.config]["seed"] + 1000 * rank
+    pr = synth.make_problem(args.config, seed=seed, **over)
+    ndte = pr.ndte
+    uobs, vobs = synth.observations(pr.na, seed=seed + 500)
+    interval = synth.ADJOINT_INTERVAL
+    fs = evp1d.FieldSet.from_problem(pr)
+    s = evp1d.EVP1D.from_problem(pr, ndte=ndte, device=local)
+    stream = torch.cuda.ExternalStream(s.stream, device=local)
+    # final velocities for the seed of the misfit
+    s.run_checkpointed(ndte, fs, interval)
+    lam = _misfit_seed(fs.uvel[: pr.na], fs.vvel[: pr.na], uobs, vobs)
+    fields = lambda: evp1d.FieldSet.from_problem(pr)
+    s.upload(fields())
+    for _ in range(args.warmup):
+        s.subcycles(ndte)
+        _adjoint_once(s, stream, ndte, interval, lam, fields)
+    s.upload(fields())
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
+    sampler = ClockSampler(gpu_id) if not args.no_clocks else None
+    if sampler:
+        sampler.__enter__()
+    t_fwd, t_rec, t_sw, t_rec0, t_sw0 = [], [], [], [], []
+    s.launch_count(reset=True)
+    for _ in range(args.steps):
+        t_fwd.append(_timed(stream, lambda: s.subcycles(ndte)))
+        a, b = _adjoint_once(s, stream, ndte, interval, lam, fields)
+        t_rec.append(a)
+        t_sw.append(b)
+        a, b = _adjoint_once(s, stream, ndte, 0, lam, fields)   # sized to memory
+        t_rec0.append(a)
+        t_sw0.append(b)
+        s.upload(fields())
+    launches = s.launch_count()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    s.upload(fields())
+    s.record_subcycles(ndte, 0)
+    info0 = s.adjoint_info()
+    s.upload(fields())
+    s.record_subcycles(ndte, interval)
+    info = s.adjoint_info()
+    s.adjoint_seed(*lam)
+    s.adjoint_sweep()
+    g = s.adjoint_gradients(("strength", "Cw", "forcex", "forcey"))
+
+    # finite differences of the bit-exact forward, 32 directions
+    rng = np.random.default_rng(seed + 7)
+    h = 1e-6
+    na = pr.na
+
+    def run(prx):
+        f = evp1d.FieldSet.from_problem(prx)
+        s.run(ndte, f)
+        return f.uvel[:na].copy(), f.vvel[:na].copy()
+
+    def central(k, d, step):
+        prp, prm = pr.copy(), pr.copy()
+        prp.f[k] = pr.f[k] + step * d
+        prm.f[k] = pr.f[k] - step * d
+        up, vp = run(prp)
+        um, vm = run(prm)
+        # summed point by point so that the difference does not cancel
+        # against the size of J
+        return float(np.sum((up - um) * (up + um - 2 * uobs) +
+                            (vp - vm) * (vp + vm - 2 * vobs))) / (2 * step)
+
+    fd_err, fd_err5 = {}, {}
+    for k in ("strength", "Cw", "forcex", "forcey"):
+        for _ in range(8):
+            d = pr.f[k] * rng.standard_normal(na)
+            ad = float(np.dot(g[k], d))
+            fd_err[k] = max(fd_err.get(k, 0.0), abs(central(k, d, h) - ad) / abs(ad))
+            fd_err5[k] = max(fd_err5.get(k, 0.0), abs(central(k, d, 1e-5) - ad) / abs(ad))
+    s.finalize()
+
+    med = statistics.median
+    units = pr.n_active * ndte
+    if rank == 0:
+        print(json.dumps({
+            "metric": ADJ_METRIC, "value": units / med(t_sw), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * med(t_sw), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, reference value ranges)",
+            "config": dict(workload_config(args.config, pr, ndte),
+                           loss="J = sum (u-u_obs)^2 + (v-v_obs)^2, u_obs, v_obs ~ N(0, 0.1)",
+                           gradients="strength, Cw, forcex, forcey",
+                           checkpoint_interval=interval),
+            "forward_ms": 1000.0 * med(t_fwd),
+            "record_ms": 1000.0 * med(t_rec),
+            "sweep_ms": 1000.0 * med(t_sw),
+            "adjoint_over_forward": med(t_sw) / med(t_fwd),
+            "gradient_over_forward": (med(t_rec) + med(t_sw)) / med(t_fwd),
+            "memory_sized": {"tape_subcycles": info0["tape_subcycles"],
+                             "interval": info0["interval"],
+                             "record_ms": 1000.0 * med(t_rec0),
+                             "sweep_ms": 1000.0 * med(t_sw0),
+                             "adjoint_over_forward": med(t_sw0) / med(t_fwd),
+                             "store_bytes": info0["store_bytes"]},
+            "memory_bytes": {"checkpoints_and_tape": info["store_bytes"],
+                             "adjoint_work": info["work_bytes"],
+                             "forward_solver": info["solver_bytes"]},
+            "fd_check": {"directions": 32, "step": h, "max_rel_err": fd_err,
+                         "max_rel_err_step_1e-5": fd_err5},
+            "gpu_launches": launches,
+            "clocks": sampler.summary() if sampler else None,
+        }), flush=True)
+
+
+def run_adjoint_batched(args, rank, world, local):
+    """The 32-member adjoint ensemble (ny = 600, nx ~ U(300, 1300), ndte =
+    1000, gradients of the misfit with respect to forcex and forcey):
+    one batched handle with memory-sized checkpoints against looping the
+    single-member adjoint; gradients compared member by member."""
+    import numpy as np
+    import torch
+    import evp1d
+    from evp1d import synth
+
+    torch.cuda.set_device(local)
+    cfg = dict(synth.ENSEMBLES[args.config])
+    if args.ndte:
+        cfg["ndte"] = args.ndte
+    cfg["seed"] += 1000 * rank
+    members = synth.make_ensemble(**cfg)
+    ndte = cfg["ndte"]
+    ens = synth.concat(members)
+    obs = [synth.observations(m.na, seed=cfg["seed"] + 500 + i) for i, m in enumerate(members)]
+    want = ("forcex", "forcey")
+    free0 = torch.cuda.mem_get_info(local)[0]
+    fs = evp1d.FieldSet.from_problem(ens.combined)
+    s = evp1d.EVP1D.batched(ens, ndte=ndte, device=local)
+    stream = torch.cuda.ExternalStream(s.stream, device=local)
+    s.run_checkpointed(ndte, fs, 0)
+    u_list = np.concatenate([u[: m.na] for u, m in zip(ens.split_slots(fs.uvel), members)])
+    v_list = np.concatenate([v[: m.na] for v, m in zip(ens.split_slots(fs.vvel), members)])
+    uobs = np.concatenate([o[0] for o in obs])
+    vobs = np.concatenate([o[1] for o in obs])
+    lam = _misfit_seed(u_list, v_list, uobs, vobs)
+    fields = lambda: evp1d.FieldSet.from_problem(ens.combined)
+    for _ in range(args.warmup):
+        _adjoint_once(s, stream, ndte, 0, lam, fields)
+    t_rec, t_sw = [], []
+    s.launch_count(reset=True)
+    for _ in range(args.steps):
+        a, b = _adjoint_once(s, stream, ndte, 0, lam, fields)
+        t_rec.append(a)
+        t_sw.append(b)
+    launches = s.launch_count()
+    peak_used = free0 - torch.cuda.mem_get_info(local)[0]
+    info = s.adjoint_info()
+    g = s.adjoint_gradients(want)
+    s.finalize()
+    # loop: one handle per member, the same work one member at a time
+    loop_rec = loop_sw = 0.0
+    worst = 0.0
+    off = 0
+    loop_peak = 0
+    for i, m in enumerate(members):
+        f1 = evp1d.FieldSet.from_problem(m)
+        h = evp1d.EVP1D.from_problem(m, ndte=ndte, device=local)
+        st = torch.cuda.ExternalStream(h.stream, device=local)
+        h.run_checkpointed(ndte, f1, 0)
+        lam_m = _misfit_seed(f1.uvel[: m.na], f1.vvel[: m.na], obs[i][0], obs[i][1])
+        fm = lambda m=m: evp1d.FieldSet.from_problem(m)
+        ts = [_adjoint_once(h, st, ndte, 0, lam_m, fm) for _ in range(args.steps)]
+        loop_rec += statistics.median([t[0] for t in ts])
+        loop_sw += statistics.median([t[1] for t in ts])
+        gi = h.adjoint_gradients(want)
+        inf = h.adjoint_info()
+        loop_peak = max(loop_peak, inf["store_bytes"] + inf["work_bytes"] + inf["solver_bytes"])
+        for k in want:
+            ref = gi[k]
+            worst = max(worst, float(np.abs(g[k][off: off + m.na] - ref).max()
+                                     / max(np.abs(ref).max(), 1e-300)))
+        h.finalize()
+        off += m.na
+    med = statistics.median
+    units = sum(m.n_active for m in members) * ndte
+    if rank == 0:
+        print(json.dumps({
+            "metric": ADJ_METRIC + " (ensemble)", "value": units / (med(t_rec) + med(t_sw)),
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * (med(t_rec) + med(t_sw)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, reference value ranges)",
+            "config": {"workload": f"evp1d {args.config}: {len(members)} members, "
+                                   f"{units // ndte} active points, ndte={ndte}, FP64 adjoint",
+                       "members": len(members), "active_points": units // ndte,
+                       "ndte": ndte, "gradients": "forcex, forcey",
+                       "checkpoints": "sized to device memory"},
+            "record_ms": 1000.0 * med(t_rec), "sweep_ms": 1000.0 * med(t_sw),
+            "loop_record_ms": 1000.0 * loop_rec, "loop_sweep_ms": 1000.0 * loop_sw,
+            "batched_vs_loop": (loop_rec + loop_sw) / (med(t_rec) + med(t_sw)),
+            "max_rel_diff_vs_loop": worst,
+            "checkpointing": {"tape_subcycles": info["tape_subcycles"],
+                              "interval": info["interval"],
+                              "checkpoints": info["checkpoints"]},
+            "memory_bytes": {"checkpoints_and_tape": info["store_bytes"],
+                             "adjoint_work": info["work_bytes"],
+                             "forward_solver": info["solver_bytes"],
+                             "device_used_peak": int(peak_used),
+                             "loop_largest_member": loop_peak},
+            "gpu_launches": launches,
+        }), flush=True)
+
+
+# --------------------------------------------------------------------------
 # GPU
 # --------------------------------------------------------------------------
 def main():
@@ -296,6 +548,12 @@ def main():
         run_reference(args, rank, world)
         return
     from evp1d import synth as _synth
+    if args.config == "cfg4":
+        run_adjoint(args, rank, world, local)
+        return
+    if args.config == "cfg5":
+        run_adjoint_batched(args, rank, world, local)
+        return
     if args.config in _synth.ENSEMBLES:
         run_ensemble(args, rank, world, local)
         return

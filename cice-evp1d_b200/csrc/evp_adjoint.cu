@@ -227,15 +227,18 @@ __global__ void __launch_bounds__(kThreads) k_adj_final(AdjArgs a, int fold_init
   }
 }
 
-// Copy the halo slots [nslots, nslots+nhs) of src into entries 1..count-1 of
-// a tape whose entries are `stride` doubles apart.
-__global__ void k_fill_halo(double *tape, size_t stride, int nslots, int nhs, int count,
-                            const double *src) {
-  const long long total = (long long)nhs * (count - 1);
+// The forward kernels write u, v only at the slots they update (U points that
+// are not skipU); the ping-pong buffers keep the constant rest.  Tape entries
+// get that constant part -- skipU and padding slots [0, nslots) and halo
+// slots [nslots, nuv) -- from src, for entries 1..count-1 of a tape whose
+// entries are `stride` doubles apart.
+__global__ void k_fill_constant(double *tape, size_t stride, int nslots, int nuv,
+                                int count, const double *src, const uint8_t *flags) {
+  const long long total = (long long)nuv * (count - 1);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int e = 1 + (int)(t / nhs), j = (int)(t % nhs);
-    tape[(size_t)e * stride + nslots + j] = src[nslots + j];
+    const int e = 1 + (int)(t / nuv), j = (int)(t % nuv);
+    if (j >= nslots || (flags[j] & kSkipU)) tape[(size_t)e * stride + j] = src[j];
   }
 }
 
@@ -266,10 +269,15 @@ struct AdjointState {
   size_t store_bytes = 0;
   size_t stride = 0;    // doubles per velocity tape entry (nuv, padded)
   size_t sstride = 0;   // doubles per stress array of a checkpoint (nslots, padded)
-  double *ck = nullptr;  // nseg checkpoints of u, v (stride each), 12 stresses
+  // Subcycles [0, n_cp) are covered by checkpoints every `interval`
+  // subcycles (nck of them) and recomputed segment by segment in the sweep;
+  // subcycles [n_cp, ndte) keep every velocity state on the tape.
+  double *ck = nullptr;    // nck checkpoints of u, v (stride each), 12 stresses
   double *tape = nullptr;  // tape entries: u then v, 2*stride doubles each
-  bool valid = false, full_tape = false, uinit_explicit = false, seeded = false;
-  int ndte = 0, interval = 0, nseg = 0;
+  int tape_entries = 0;
+  bool valid = false, uinit_explicit = false, seeded = false;
+  int ndte = 0, interval = 0, nck = 0, n_cp = 0;
+  long long budget = 0;  // bytes for checkpoints and tape (0: 80% of free memory)
   long long launches = 0;
 };
 
@@ -476,7 +484,8 @@ int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
     h->adj->device = d.device;
     h->adj->valid = true;
     h->adj->ndte = ndte;
-    h->adj->nseg = 0;
+    h->adj->nck = 0;
+    h->adj->n_cp = 0;
     h->adj->seeded = false;
     return EVP1D_OK;
   }
@@ -488,81 +497,81 @@ int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
   A.sstride = pad256((size_t)d.nslots);
   const size_t entry = 2 * A.stride * sizeof(double);
   const size_t ckpt = (2 * A.stride + 12 * A.sstride) * sizeof(double);
-  bool full = false;
-  if (interval <= 0) {
+  // split of the subcycles into a checkpointed head and a taped tail
+  int k = 0, n_cp = 0;
+  if (interval > 0) {
+    k = std::min(interval, ndte);
+    n_cp = ndte;
+  } else {
     size_t freeb = 0, totalb = 0;
     ADJ_TRY(cudaMemGetInfo(&freeb, &totalb));
-    const size_t have = freeb + (A.store ? A.store_bytes : 0);
-    if ((size_t)(ndte + 1) * entry <= have / 2) {
-      full = true;
-    } else {
-      // fixed-interval checkpoints with the memory-minimising interval
-      // sqrt(ndte * checkpoint / tape entry)
-      interval = (int)std::ceil(std::sqrt((double)ndte * (double)ckpt / (double)entry));
-      interval = std::max(1, std::min(interval, ndte));
+    const double budget = A.budget > 0 ? (double)A.budget
+                                       : 0.8 * (double)(freeb + A.store_bytes);
+    if ((double)(ndte + 1) * (double)entry > budget) {
+      // interval sqrt(ndte * checkpoint / tape entry) minimises the memory of
+      // a checkpoints-only recording; the rest of the budget tapes the tail
+      k = (int)std::ceil(std::sqrt((double)ndte * (double)ckpt / (double)entry));
+      k = std::max(1, std::min(k, ndte));
+      const double nck_max = std::ceil((double)ndte / k);
+      double entries = std::floor((budget - nck_max * (double)ckpt) / (double)entry);
+      entries = std::max(entries, (double)(k + 1));
+      n_cp = std::max(0, ndte - ((int)std::min(entries, (double)(ndte + 1)) - 1));
+      if (n_cp == 0) k = 0;
     }
   }
+  const int nck = n_cp > 0 ? (n_cp + k - 1) / k : 0;
+  const int entries = std::max(ndte - n_cp + 1, n_cp > 0 ? k + 1 : 0);
+  ADJ_CHECK(ensure_store(A, (size_t)nck * ckpt + (size_t)entries * entry));
+  A.ck = (double *)A.store;
+  A.tape = A.ck + (size_t)nck * (ckpt / sizeof(double));
+  A.tape_entries = entries;
+  A.interval = k;
+  A.nck = nck;
+  A.n_cp = n_cp;
   cudaStream_t st = d.stream;
   const int cur0 = d.cur;
-  if (full) {
-    ADJ_CHECK(ensure_store(A, (size_t)(ndte + 1) * entry));
-    A.tape = (double *)A.store;
-    A.ck = nullptr;
-    A.full_tape = true;
-    A.interval = ndte;
-    A.nseg = 1;
-    ADJ_TRY(cudaMemcpyAsync(tape_u(A, 0), d.u[cur0], sizeof(double) * d.nuv,
+  // the constant slots of every tape entry (entry 0 is copied whole each time)
+  if (entries > 1) {
+    const long long work = (long long)d.nuv * (entries - 1);
+    k_fill_constant<<<blocks_for(work), kThreads, 0, st>>>(
+        A.tape, 2 * A.stride, d.nslots, d.nuv, entries, d.u[cur0], d.flags);
+    k_fill_constant<<<blocks_for(work), kThreads, 0, st>>>(
+        A.tape + A.stride, 2 * A.stride, d.nslots, d.nuv, entries, d.v[cur0], d.flags);
+  }
+  // checkpointed head: the ordinary subcycle loop with a copy of the state
+  // at the start of every segment
+  for (int j = 0; j < nck; j++) {
+    const int c = d.cur;
+    ADJ_TRY(cudaMemcpyAsync(ck_u(A, j), d.u[c], sizeof(double) * d.nuv,
                             cudaMemcpyDeviceToDevice, st));
-    ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), d.v[cur0], sizeof(double) * d.nuv,
+    ADJ_TRY(cudaMemcpyAsync(ck_v(A, j), d.v[c], sizeof(double) * d.nuv,
                             cudaMemcpyDeviceToDevice, st));
-    if (d.nhs > 0) {
-      k_fill_halo<<<blocks_for((long long)d.nhs * ndte), kThreads, 0, st>>>(
-          A.tape, 2 * A.stride, d.nslots, d.nhs, ndte + 1, d.u[cur0]);
-      k_fill_halo<<<blocks_for((long long)d.nhs * ndte), kThreads, 0, st>>>(
-          A.tape + A.stride, 2 * A.stride, d.nslots, d.nhs, ndte + 1, d.v[cur0]);
-    }
-    int b = cur0;
-    for (int n = 0; n < ndte; n++) {
-      launch_state(h, d.stress[b], d.stress[1 - b], tape_u(A, n), tape_v(A, n),
-                   tape_u(A, n + 1), tape_v(A, n + 1), n == ndte - 1);
+    for (int q = 0; q < 12; q++)
+      ADJ_TRY(cudaMemcpyAsync(ck_s(A, j, q), d.stress[c][q], sizeof(double) * d.nslots,
+                              cudaMemcpyDeviceToDevice, st));
+    ADJ_CHECK(evp1d_subcycles(h, std::min(k, n_cp - j * k)));
+  }
+  // taped tail: each subcycle writes its velocities into the next entry
+  if (n_cp < ndte) {
+    const int c = d.cur;
+    ADJ_TRY(cudaMemcpyAsync(tape_u(A, 0), d.u[c], sizeof(double) * d.nuv,
+                            cudaMemcpyDeviceToDevice, st));
+    ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), d.v[c], sizeof(double) * d.nuv,
+                            cudaMemcpyDeviceToDevice, st));
+    int b = c;
+    for (int n = n_cp; n < ndte; n++) {
+      const int e = n - n_cp;
+      launch_state(h, d.stress[b], d.stress[1 - b], tape_u(A, e), tape_v(A, e),
+                   tape_u(A, e + 1), tape_v(A, e + 1), n == ndte - 1);
       b = 1 - b;
     }
-    h->launches += ndte;
+    h->launches += ndte - n_cp;
     // the final state back into the handle's buffers for evp1d_download
-    ADJ_TRY(cudaMemcpyAsync(d.u[b], tape_u(A, ndte), sizeof(double) * d.nslots,
+    ADJ_TRY(cudaMemcpyAsync(d.u[b], tape_u(A, ndte - n_cp), sizeof(double) * d.nslots,
                             cudaMemcpyDeviceToDevice, st));
-    ADJ_TRY(cudaMemcpyAsync(d.v[b], tape_v(A, ndte), sizeof(double) * d.nslots,
+    ADJ_TRY(cudaMemcpyAsync(d.v[b], tape_v(A, ndte - n_cp), sizeof(double) * d.nslots,
                             cudaMemcpyDeviceToDevice, st));
     d.cur = b;
-  } else {
-    const int k = interval;
-    const int nseg = (ndte + k - 1) / k;
-    const size_t bytes = (size_t)nseg * ckpt + (size_t)(k + 1) * entry;
-    ADJ_CHECK(ensure_store(A, bytes));
-    A.ck = (double *)A.store;
-    A.tape = A.ck + (size_t)nseg * (ckpt / sizeof(double));
-    A.full_tape = false;
-    A.interval = k;
-    A.nseg = nseg;
-    // halo slots of the segment tape (entry 0 comes with each checkpoint)
-    if (d.nhs > 0 && k > 0) {
-      k_fill_halo<<<blocks_for((long long)d.nhs * k), kThreads, 0, st>>>(
-          A.tape, 2 * A.stride, d.nslots, d.nhs, k + 1, d.u[cur0]);
-      k_fill_halo<<<blocks_for((long long)d.nhs * k), kThreads, 0, st>>>(
-          A.tape + A.stride, 2 * A.stride, d.nslots, d.nhs, k + 1, d.v[cur0]);
-    }
-    for (int j = 0; j < nseg; j++) {
-      const int c = d.cur;
-      ADJ_TRY(cudaMemcpyAsync(ck_u(A, j), d.u[c], sizeof(double) * d.nuv,
-                              cudaMemcpyDeviceToDevice, st));
-      ADJ_TRY(cudaMemcpyAsync(ck_v(A, j), d.v[c], sizeof(double) * d.nuv,
-                              cudaMemcpyDeviceToDevice, st));
-      for (int q = 0; q < 12; q++)
-        ADJ_TRY(cudaMemcpyAsync(ck_s(A, j, q), d.stress[c][q], sizeof(double) * d.nslots,
-                                cudaMemcpyDeviceToDevice, st));
-      const int len = std::min(k, ndte - j * k);
-      ADJ_CHECK(evp1d_subcycles(h, len));
-    }
   }
   ADJ_TRY(cudaGetLastError());
   A.ndte = ndte;
@@ -640,30 +649,31 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
     k_adj_stress<<<grid, kThreads, 0, st>>>(a, h->p, u0, v0);
     launches += 2;
   };
-  if (A.full_tape) {
-    for (int n = A.ndte - 1; n >= 0; n--)
-      reverse_step(tape_u(A, n), tape_v(A, n), tape_u(A, n + 1), tape_v(A, n + 1));
-  } else {
-    const int k = A.interval;
-    for (int j = A.nseg - 1; j >= 0; j--) {
-      const int len = std::min(k, A.ndte - j * k);
-      ADJ_TRY(cudaMemcpyAsync(tape_u(A, 0), ck_u(A, j), sizeof(double) * d.nuv,
+  // taped tail
+  for (int n = A.ndte - 1; n >= A.n_cp; n--) {
+    const int e = n - A.n_cp;
+    reverse_step(tape_u(A, e), tape_v(A, e), tape_u(A, e + 1), tape_v(A, e + 1));
+  }
+  // checkpointed head, one segment at a time from the last
+  const int k = A.interval;
+  for (int j = A.nck - 1; j >= 0; j--) {
+    const int len = std::min(k, A.n_cp - j * k);
+    ADJ_TRY(cudaMemcpyAsync(tape_u(A, 0), ck_u(A, j), sizeof(double) * d.nuv,
+                            cudaMemcpyDeviceToDevice, st));
+    ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), ck_v(A, j), sizeof(double) * d.nuv,
+                            cudaMemcpyDeviceToDevice, st));
+    for (int q = 0; q < 12; q++)
+      ADJ_TRY(cudaMemcpyAsync(A.spp[0][q], ck_s(A, j, q), sizeof(double) * d.nslots,
                               cudaMemcpyDeviceToDevice, st));
-      ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), ck_v(A, j), sizeof(double) * d.nuv,
-                              cudaMemcpyDeviceToDevice, st));
-      for (int q = 0; q < 12; q++)
-        ADJ_TRY(cudaMemcpyAsync(A.spp[0][q], ck_s(A, j, q), sizeof(double) * d.nslots,
-                                cudaMemcpyDeviceToDevice, st));
-      // recompute the segment's velocities from its checkpoint
-      for (int i = 0; i < len; i++) {
-        const int b = i & 1;
-        launch_state(h, A.spp[b], A.spp[1 - b], tape_u(A, i), tape_v(A, i),
-                     tape_u(A, i + 1), tape_v(A, i + 1), false);
-        launches++;
-      }
-      for (int i = len - 1; i >= 0; i--)
-        reverse_step(tape_u(A, i), tape_v(A, i), tape_u(A, i + 1), tape_v(A, i + 1));
+    // recompute the segment's velocities from its checkpoint
+    for (int i = 0; i < len; i++) {
+      const int b = i & 1;
+      launch_state(h, A.spp[b], A.spp[1 - b], tape_u(A, i), tape_v(A, i), tape_u(A, i + 1),
+                   tape_v(A, i + 1), false);
+      launches++;
     }
+    for (int i = len - 1; i >= 0; i--)
+      reverse_step(tape_u(A, i), tape_v(A, i), tape_u(A, i + 1), tape_v(A, i + 1));
   }
   k_adj_final<<<grid, kThreads, 0, st>>>(a, A.uinit_explicit ? 0 : 1);
   launches++;
@@ -734,15 +744,25 @@ int evp1d_adjoint(evp1d_t *h, const double *lam_uvel, const double *lam_vvel,
   return evp1d_adjoint_gradients(h, g);
 }
 
+int evp1d_set_adjoint_budget(evp1d_t *h, long long bytes) {
+  if (!h || bytes < 0) return error(EVP1D_ERR_INVALID_ARG, "bad arguments");
+  if (!h->adj) {
+    h->adj = new AdjointState();
+    h->adj->device = h->d.device;
+  }
+  h->adj->budget = bytes;
+  return EVP1D_OK;
+}
+
 int evp1d_adjoint_info(evp1d_t *h, long long info[8]) {
   if (!h || !info) return error(EVP1D_ERR_INVALID_ARG, "NULL argument");
   for (int k = 0; k < 8; k++) info[k] = 0;
   const AdjointState *A = h->adj;
   if (!A) return EVP1D_OK;
   info[0] = A->valid ? 1 : 0;
-  info[1] = A->full_tape ? 1 : 0;
+  info[1] = A->ndte - A->n_cp;
   info[2] = A->interval;
-  info[3] = A->nseg;
+  info[3] = A->nck;
   info[4] = (long long)A->store_bytes;
   info[5] = (long long)A->arena_bytes;
   info[6] = (long long)h->d.arena_bytes;

@@ -304,9 +304,15 @@ class EVP1D:
     def adjoint_info(self) -> dict:
         info = (C.c_longlong * 8)()
         check(self._L.evp1d_adjoint_info(self.h, info), "evp1d_adjoint_info")
-        keys = ("valid", "full_tape", "interval", "segments", "store_bytes",
+        keys = ("valid", "tape_subcycles", "interval", "checkpoints", "store_bytes",
                 "work_bytes", "solver_bytes", "sweep_launches")
         return {k: int(v) for k, v in zip(keys, info)}
+
+    def set_adjoint_budget(self, nbytes: int) -> None:
+        """Device memory for the checkpoints and tape of sized recordings
+        (interval 0); 0 = 80% of the free memory."""
+        check(self._L.evp1d_set_adjoint_budget(self.h, int(nbytes)),
+              "evp1d_set_adjoint_budget")
 
     def set_params(self, params: Params) -> None:
         check(self._L.evp1d_set_params(self.h, C.byref(params)), "evp1d_set_params")

@@ -115,9 +115,10 @@ def load() -> C.CDLL:
     L.evp1d_adjoint_sweep.argtypes = [H]
     L.evp1d_adjoint_gradients.argtypes = [H, C.POINTER(Grads)]
     L.evp1d_adjoint_info.argtypes = [H, C.POINTER(C.c_longlong)]
+    L.evp1d_set_adjoint_budget.argtypes = [H, C.c_longlong]
     for name in ("evp1d_run_checkpointed", "evp1d_record_subcycles", "evp1d_adjoint",
                  "evp1d_adjoint_seed", "evp1d_adjoint_sweep", "evp1d_adjoint_gradients",
-                 "evp1d_adjoint_info"):
+                 "evp1d_adjoint_info", "evp1d_set_adjoint_budget"):
         getattr(L, name).restype = C.c_int
     L.evp1d_run_device_noalloc.argtypes = ([C.c_int, C.c_int] + [C.c_void_p] * 13
                                            + [C.POINTER(Params), C.c_int,

@@ -254,11 +254,14 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
  *      interval > 0:  (u, v, 12 stresses) every `interval` subcycles; the
  *                     sweep recomputes each segment's velocities from its
  *                     checkpoint (one extra forward in all);
- *      interval <= 0: sized to device memory: every subcycle's velocities
- *                     when they fit in half of the free memory (no
- *                     recompute), else checkpoints at the interval
- *                     ceil(sqrt(ndte * checkpoint size / velocity size)),
- *                     which minimises memory.
+ *      interval <= 0: sized to device memory (the budget of
+ *                     evp1d_set_adjoint_budget, default 80% of the free
+ *                     memory): every subcycle's velocities when they fit (no
+ *                     recompute); else checkpoints at the interval
+ *                     ceil(sqrt(ndte * checkpoint size / velocity size)) for
+ *                     the first subcycles and every velocity state for as
+ *                     many final subcycles as the budget holds, so only the
+ *                     checkpointed head is recomputed.
  * 2. evp1d_adjoint: given dJ/d uvel, dJ/d vvel of the call's final list-point
  *    velocities ([na], host) and optionally dJ/d of the final stresses
  *    (lam_stress: NULL, or 12 pointers of which any may be NULL), writes the
@@ -292,10 +295,15 @@ int evp1d_adjoint_seed(evp1d_t *handle, const double *lam_uvel, const double *la
                        const double *const *lam_stress);
 int evp1d_adjoint_sweep(evp1d_t *handle);
 int evp1d_adjoint_gradients(evp1d_t *handle, const evp1d_grads *grads);
-/* info[0] 1 if a recorded forward is held, [1] 1 for a full velocity tape,
- * [2] checkpoint interval, [3] segments, [4] bytes of checkpoints and tape,
- * [5] bytes of the adjoint work arrays, [6] bytes of the forward solver,
- * [7] kernel launches of the last sweep. */
+/* Device memory for checkpoints and tape of later sized recordings
+ * (interval <= 0); 0 restores the default, 80% of the free memory.  A
+ * budget below what checkpointing at the memory-minimising interval needs
+ * gets that minimum. */
+int evp1d_set_adjoint_budget(evp1d_t *handle, long long bytes);
+/* info[0] 1 if a recorded forward is held, [1] subcycles on the velocity
+ * tape (the final ones), [2] checkpoint interval, [3] checkpoints, [4] bytes
+ * of checkpoints and tape, [5] bytes of the adjoint work arrays, [6] bytes of
+ * the forward solver, [7] kernel launches of the last sweep. */
 int evp1d_adjoint_info(evp1d_t *handle, long long info[8]);
 
 /* ----------------------------------------------------------------------------

@@ -50,7 +50,7 @@ def test_adjoint_matches_tape(oracle_mod, curvilinear, interval):
     p = evp1d.set_evp_parameters(ndte)
     g, fs, info = gpu_grads(pr, ndte, uobs, vobs, interval=interval, stress=True)
     assert info["valid"] == 1
-    assert info["full_tape"] == (1 if interval == 0 else 0)
+    assert info["tape_subcycles"] == (ndte if interval == 0 else 0)
     t = evp_tape.gradient(pr, ndte, p, uobs, vobs)
     for k in FIELDS:
         assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
@@ -81,9 +81,62 @@ def test_checkpoint_and_tape_sweeps_agree_bitwise():
     ga, _, ia = gpu_grads(pr, pr.ndte, uobs, vobs, interval=0)
     for interval in (1, 7, 31, 100):
         gb, _, ib = gpu_grads(pr, pr.ndte, uobs, vobs, interval=interval)
-        assert ib["segments"] == -(-pr.ndte // min(interval, 100))
+        assert ib["checkpoints"] == -(-pr.ndte // min(interval, pr.ndte))
         for k in ga:
             assert np.array_equal(ga[k].view(np.int64), gb[k].view(np.int64)), (interval, k)
+
+
+def test_recordings_on_one_handle_and_constant_slots(oracle_mod):
+    """Velocities at skipU points stay at their starting value through the
+    call and enter the stress of neighbouring T points; with them nonzero,
+    recordings of different layouts in a row on one handle (full tape, then
+    checkpoints, then the tape again) give each mode's fresh-handle gradients
+    bit for bit, and these match the tape oracle."""
+    import evp_tape
+    pr = small(seed=44, ndte=24)
+    rng = np.random.default_rng(2)
+    su = pr.skipU != 0
+    assert su.any()
+    pr.uvel[: pr.na][su] = rng.normal(0, 0.05, su.sum())
+    pr.vvel[: pr.na][su] = rng.normal(0, 0.05, su.sum())
+    pr.f["uvel_init"] = pr.uvel[: pr.na].copy()
+    pr.f["vvel_init"] = pr.vvel[: pr.na].copy()
+    uobs, vobs = synth.observations(pr.na, seed=9)
+    fresh = {iv: gpu_grads(pr, pr.ndte, uobs, vobs, interval=iv)[0] for iv in (0, 5)}
+    t = evp_tape.gradient(pr, pr.ndte, evp1d.set_evp_parameters(pr.ndte), uobs, vobs,
+                          wrt=FIELDS)
+    for k in FIELDS:
+        assert rel(fresh[0][k], t[k]) < 1e-9, k
+    with evp1d.EVP1D.from_problem(pr) as s:
+        for iv in (0, 5, 0, 5):
+            fs = evp1d.FieldSet.from_problem(pr)
+            s.run_checkpointed(pr.ndte, fs, iv)
+            g = s.adjoint(2 * (fs.uvel[: pr.na] - uobs), 2 * (fs.vvel[: pr.na] - vobs))
+            for k in g:
+                assert np.array_equal(g[k].view(np.int64), fresh[iv][k].view(np.int64)), (iv, k)
+
+
+def test_memory_sized_recording_with_a_small_budget():
+    """A budget of 45 velocity-tape entries (of 61): the first subcycles are
+    checkpointed and recomputed, the final ones taped; the forward outputs
+    and the gradients are those of the full tape, bit for bit."""
+    pr = small(seed=46, ndte=60)
+    uobs, vobs = synth.observations(pr.na, seed=4)
+    ga, fa, ia = gpu_grads(pr, pr.ndte, uobs, vobs, interval=0)
+    assert ia["tape_subcycles"] == pr.ndte
+    entry = ia["store_bytes"] // (pr.ndte + 1)
+    fs = evp1d.FieldSet.from_problem(pr)
+    with evp1d.EVP1D.from_problem(pr) as s:
+        s.set_adjoint_budget(entry * 45)
+        s.run_checkpointed(pr.ndte, fs, 0)
+        info = s.adjoint_info()
+        g = s.adjoint(2 * (fs.uvel[: pr.na] - uobs), 2 * (fs.vvel[: pr.na] - vobs))
+    assert 0 < info["tape_subcycles"] < pr.ndte and info["checkpoints"] > 0, info
+    assert info["store_bytes"] <= entry * 45
+    for a, b in ((fs.uvel, fa.uvel), (fs.vvel, fa.vvel), (fs.stress, fa.stress)):
+        assert np.array_equal(a.view(np.int64), b.view(np.int64))
+    for k in ga:
+        assert np.array_equal(ga[k].view(np.int64), g[k].view(np.int64)), k
 
 
 def central_difference(run, pr, field, d, h, uobs, vobs):
