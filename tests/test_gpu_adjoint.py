@@ -253,3 +253,40 @@ def test_adjoint_state_errors():
         with pytest.raises(evp1d.EVP1DError) as e:
             s.adjoint(z, z)
         assert e.value.code == -7
+
+
+def test_autograd_function_gradcheck():
+    """torch.autograd.gradcheck of the library's adjoint (through the
+    autograd binding) on a small problem: the full Jacobian of the final
+    velocities with respect to the four fields against torch's numerical
+    Jacobian of the GPU forward."""
+    import torch
+    from evp1d.autograd import evp_velocities
+    pr = small(seed=55, nx=13, ny=11, ndte=6)
+    with evp1d.EVP1D.from_problem(pr) as s:
+        ins = tuple(torch.tensor(pr.f[k], dtype=torch.float64, requires_grad=True)
+                    for k in ("strength", "Cw", "forcex", "forcey"))
+        # relative perturbations: scale each input to order one
+        scale = [float(np.abs(pr.f[k]).max()) or 1.0 for k in ("strength", "Cw", "forcex", "forcey")]
+        xs = tuple((t / c).detach().requires_grad_(True) for t, c in zip(ins, scale))
+
+        def f(a, b, c, d):
+            return evp_velocities(s, pr, pr.ndte, a * scale[0], b * scale[1], c * scale[2],
+                                  d * scale[3], interval=2)
+        assert torch.autograd.gradcheck(f, xs, eps=1e-6, atol=1e-7, rtol=1e-4)
+
+
+def test_autograd_function_matches_tape(oracle_mod):
+    import torch
+    import evp_tape
+    from evp1d.autograd import evp_velocities
+    pr = small(seed=57, ndte=10)
+    uobs, vobs = synth.observations(pr.na, seed=11)
+    with evp1d.EVP1D.from_problem(pr) as s:
+        ins = [torch.tensor(pr.f[k], dtype=torch.float64, requires_grad=True) for k in FIELDS]
+        u, v = evp_velocities(s, pr, pr.ndte, *ins)
+        J = ((u - torch.from_numpy(uobs)) ** 2 + (v - torch.from_numpy(vobs)) ** 2).sum()
+        J.backward()
+    t = evp_tape.gradient(pr, pr.ndte, evp1d.set_evp_parameters(pr.ndte), uobs, vobs, wrt=FIELDS)
+    for k, x in zip(FIELDS, ins):
+        assert rel(x.grad.numpy(), t[k]) < 1e-9, k
