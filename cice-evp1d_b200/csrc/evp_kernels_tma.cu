@@ -170,10 +170,17 @@ __device__ __forceinline__ void trace_stamp(const TmaArgs &a, int it, int slot) 
 // ---------------- the kernel ---------------------------------------------------
 template <bool kLast>
 __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
-  extern __shared__ unsigned char smem_raw[];
-  Smem &S = *reinterpret_cast<Smem *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  // Indexed straight off the __shared__ symbol (no integer round trip), so
+  // every access compiles to a shared-memory load or store, not a generic one.
+  // The bulk copies need 16-byte alignment, which the dynamic shared memory
+  // base has (checked: a misaligned base is refused, not faulted on).
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
   const int tid = threadIdx.x;
+  if (smem_addr(smem_raw) & 15u) {
+    if (tid == 0) atomicMax(a.err, 8);
+    return;
+  }
   if (tid == 0) {
     for (int s = 0; s < kStages; s++) {
       mbar_init(&S.full[s], 1 + 32);  // expect_tx arrival + 32 cp.async lanes
@@ -409,7 +416,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   }
 }
 
-size_t smem_bytes() { return sizeof(Smem) + 128; }
+size_t smem_bytes() { return sizeof(Smem); }
 
 }  // namespace
 
