@@ -42,8 +42,8 @@ __device__ bool wait(unsigned long long *b, uint32_t par, int *err) {
   return true;
 }
 
-__global__ void k_bulk(const char *src, size_t field_stride, int ntiles, int ncopies,
-                       int copy_bytes, int stages, int *err) {
+__global__ void k_bulk(const char *src, size_t field_stride, int ntiles, int nt_field,
+                       int ncopies, int copy_bytes, int stages, int *err) {
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned long long *full = reinterpret_cast<unsigned long long *>(sm);
   unsigned long long *empty = full + 8;
@@ -77,7 +77,7 @@ __global__ void k_bulk(const char *src, size_t field_stride, int ntiles, int nco
                      : "memory");
       __syncwarp();
       for (int k = lane; k < ncopies; k += 32) {
-        const char *g = src + (size_t)k * field_stride + (size_t)t * copy_bytes;
+        const char *g = src + (size_t)k * field_stride + (size_t)(t % nt_field) * copy_bytes;
         unsigned char *d = buf + (size_t)s * tile_bytes + (size_t)k * copy_bytes;
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
@@ -124,25 +124,32 @@ int main() {
       {1, 73728, 2}, {4, 18432, 2}, {9, 8192, 2},      // the same bytes in fewer copies
       {18, 2048, 2}, {18, 2048, 4}, {18, 2048, 6},     // half tiles, more stages
       {36, 1024, 2}, {36, 1024, 4}, {36, 1024, 5},     // 128-point tiles
+      {36, 2048, -1}, {36, 2048, -2}, {1, 73728, -1},  // from L2
   };
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   printf("copies x bytes, stages, tile KB, GB/s (whole GPU), per SM GB/s\n");
   for (const Shape &sh : shapes) {
-    // field arrays start on 256-byte boundaries (bulk copies need 16)
-    const size_t field_stride = (total / (size_t)sh.ncopies) & ~(size_t)255;
-    const int ntiles = (int)(field_stride / (size_t)sh.copy_bytes);
-    const int smem = 128 + sh.stages * sh.ncopies * sh.copy_bytes;
+    // field arrays start on 256-byte boundaries (bulk copies need 16); a
+    // negative stage count reads a 24 MB window again and again (L2 hits)
+    const bool l2 = sh.stages < 0;
+    const int stages = l2 ? -sh.stages : sh.stages;
+    const size_t span = l2 ? ((size_t)24 << 20) : total;
+    const size_t field_stride = (span / (size_t)sh.ncopies) & ~(size_t)255;
+    const int nt_field = (int)(field_stride / (size_t)sh.copy_bytes);
+    const int ntiles = l2 ? nt_field * 64 : nt_field;
+    const int smem = 128 + stages * sh.ncopies * sh.copy_bytes;
     if (cudaFuncSetAttribute(k_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
         cudaSuccess) {
       printf("%d x %d, %d stages: shared memory %d not available\n", sh.ncopies, sh.copy_bytes,
-             sh.stages, smem);
+             stages, smem);
       continue;
     }
     for (int rep = 0; rep < 2; rep++) {
       cudaEventRecord(e0);
-      k_bulk<<<sms, 64, smem>>>(src, field_stride, ntiles, sh.ncopies, sh.copy_bytes, sh.stages, err);
+      k_bulk<<<sms, 64, smem>>>(src, field_stride, ntiles, nt_field, sh.ncopies, sh.copy_bytes,
+                                stages, err);
       cudaEventRecord(e1);
       cudaEventSynchronize(e1);
     }
@@ -152,8 +159,8 @@ int main() {
     cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost);
     const cudaError_t ce = cudaGetLastError();
     const double bytes = (double)ntiles * sh.ncopies * sh.copy_bytes;
-    printf("%2d x %6d, %d stages, %6.1f KB: %7.0f GB/s  %5.1f per SM%s%s\n", sh.ncopies,
-           sh.copy_bytes, sh.stages, sh.ncopies * sh.copy_bytes / 1024.0, bytes / ms / 1e6,
+    printf("%2d x %6d, %d stages%s, %6.1f KB: %7.0f GB/s  %5.1f per SM%s%s\n", sh.ncopies,
+           sh.copy_bytes, stages, l2 ? " (L2)" : "", sh.ncopies * sh.copy_bytes / 1024.0, bytes / ms / 1e6,
            bytes / ms / 1e6 / sms, herr ? "  (a wait timed out)" : "",
            ce != cudaSuccess ? cudaGetErrorString(ce) : "");
     if (herr || ce != cudaSuccess) break;
