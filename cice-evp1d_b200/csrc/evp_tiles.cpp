@@ -27,6 +27,27 @@ const int kDJ[6] = {0, -1, -1, 0, +1, +1};
 
 inline int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
+// Position of (x, y) along the Hilbert curve filling the n x n square (n a
+// power of two), by the standard rotate-and-reflect walk over the quadrant
+// bits (the published xy-to-d conversion).
+uint64_t hilbert_index(uint32_t n, uint32_t x, uint32_t y) {
+  uint64_t d = 0;
+  for (uint32_t s = n / 2; s > 0; s /= 2) {
+    const uint32_t rx = (x & s) ? 1u : 0u, ry = (y & s) ? 1u : 0u;
+    d += (uint64_t)s * (uint64_t)s * ((3u * rx) ^ ry);
+    if (ry == 0) {
+      if (rx == 1) {
+        x = s - 1 - x;
+        y = s - 1 - y;
+      }
+      const uint32_t t = x;
+      x = y;
+      y = t;
+    }
+  }
+  return d;
+}
+
 bool reconstruct_coords(int na, const int32_t *const nb0[6],
                         std::vector<int32_t> &ci, std::vector<int32_t> &cj,
                         std::vector<int32_t> &comp) {
@@ -115,35 +136,44 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
       ci[p] -= mi[comp[p]];
       cj[p] -= mj[comp[p]];
     }
+    // pieces in a canonical order (by their position in the grid walk's
+    // coordinates is not canonical, so by size and extent), points of a piece
+    // along a Hilbert curve over its coordinates, then consecutive runs of
+    // kTileOwned points: compact, full tiles.  A run may span two pieces;
+    // pieces never share neighbours, so that only merges small floes.
+    std::vector<int32_t> pn((size_t)nc, 0), pw((size_t)nc, 0), ph((size_t)nc, 0);
+    for (int p = 0; p < na; p++) {
+      pn[comp[p]]++;
+      pw[comp[p]] = ci[p] + 1 > pw[comp[p]] ? ci[p] + 1 : pw[comp[p]];
+      ph[comp[p]] = cj[p] + 1 > ph[comp[p]] ? cj[p] + 1 : ph[comp[p]];
+    }
+    std::vector<uint64_t> hkey((size_t)na);
+    for (int p = 0; p < na; p++) {
+      uint32_t n = 1;
+      const int32_t ext = pw[comp[p]] > ph[comp[p]] ? pw[comp[p]] : ph[comp[p]];
+      while ((int64_t)n < ext) n *= 2;
+      hkey[p] = hilbert_index(n, (uint32_t)ci[p], (uint32_t)cj[p]);
+    }
+    // canonical piece order: larger first, then by extent and the first
+    // point's Hilbert position -- none of which depends on the list order
+    std::vector<uint64_t> pfirst((size_t)nc, UINT64_MAX);
+    for (int p = 0; p < na; p++) pfirst[comp[p]] = hkey[p] < pfirst[comp[p]] ? hkey[p] : pfirst[comp[p]];
     std::vector<int32_t> order((size_t)na);
     for (int p = 0; p < na; p++) order[p] = p;
-    auto key = [&](int p, int &tj, int &ti) {
-      tj = floor_div(cj[p], kTileH);
-      ti = floor_div(ci[p], kTileW);
-    };
     std::sort(order.begin(), order.end(), [&](int a, int b) {
-      int tja, tia, tjb, tib;
-      key(a, tja, tia);
-      key(b, tjb, tib);
-      if (comp[a] != comp[b]) return comp[a] < comp[b];
-      if (tja != tjb) return tja < tjb;
-      if (tia != tib) return tia < tib;
-      if (cj[a] != cj[b]) return cj[a] < cj[b];
-      return ci[a] < ci[b];
-    });
-    int k = 0;
-    while (k < na) {
-      int tj0, ti0;
-      key(order[k], tj0, ti0);
-      const int c0 = comp[order[k]];
-      std::vector<int32_t> g;
-      while (k < na) {
-        int tj, ti;
-        key(order[k], tj, ti);
-        if (comp[order[k]] != c0 || tj != tj0 || ti != ti0) break;
-        g.push_back(order[k]);
-        k++;
+      const int A = comp[a], B = comp[b];
+      if (A != B) {
+        if (pn[A] != pn[B]) return pn[A] > pn[B];
+        if (pw[A] != pw[B]) return pw[A] < pw[B];
+        if (ph[A] != ph[B]) return ph[A] < ph[B];
+        if (pfirst[A] != pfirst[B]) return pfirst[A] < pfirst[B];
+        return A < B;
       }
+      return hkey[a] < hkey[b];
+    });
+    for (int k = 0; k < na; k += kTileOwned) {
+      std::vector<int32_t> g(order.begin() + k,
+                             order.begin() + (k + kTileOwned < na ? k + kTileOwned : na));
       groups.push_back(std::move(g));
     }
   } else {

@@ -13,10 +13,12 @@ def stats(pr):
     return evp1d.plan_stats(pr.na, pr.navel, pr.idx)
 
 
-def test_cfg1_plan_uses_grid_tiles():
-    s = stats(synth.make_problem("cfg1"))
-    # 16 x 16 tiles: forward halo is one column, one row and a corner
-    assert s["from_coords"] and s["max_halo"] <= 16 + 16 + 1 and s["max_tile"] <= 256
+def test_cfg1_plan_uses_full_compact_tiles():
+    pr = synth.make_problem("cfg1")
+    s = stats(pr)
+    # Hilbert-curve runs of 256 points: tiles nearly full, forward halo small
+    assert s["from_coords"] and s["max_halo"] <= 64 and s["max_tile"] <= 256
+    assert pr.na / s["tiles"] > 0.9 * 256
     assert s["halo"] < 0.2 * s["slots"]
 
 
@@ -39,8 +41,8 @@ def test_random_graph_falls_back(na, nhalo, seed):
 
 def test_standalone_plan():
     s = stats(helpers.standalone_problem())
-    # 21 x 21 square in 16 x 16 tiles: at most 2 x 2 tiles
-    assert s["from_coords"] and s["tiles"] <= 4 and s["slots"] >= 441
+    # 441 points in runs of 256: two tiles
+    assert s["from_coords"] and s["tiles"] == 2 and s["slots"] >= 441
 
 
 def test_empty_plan():
