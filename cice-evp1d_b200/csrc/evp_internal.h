@@ -44,6 +44,7 @@ struct DeviceProblem {
   int32_t *uvx_off = nullptr, *uvx_cnt = nullptr, *uvx_idx = nullptr;
   int32_t *tile_meta = nullptr;  // 8 int32 per tile (see TmaArgs)
   int32_t *tile_rec = nullptr;   // kRecInts int32 per tile (producer records)
+  double *cblk = nullptr;        // per-call constants, kConstFields x 256 per tile
   int *err = nullptr;        // device error word of the bounded waits
   int nctas = 0;             // persistent grid size (SM count)
   uint8_t *flags = nullptr;
@@ -67,6 +68,9 @@ void problem_destroy(DeviceProblem *d);
 // uvel_init/vvel_init default to the uploaded velocities; the drag factor
 // (aiu*rhow)*Cw is precomputed; cur = 0.
 int problem_upload(DeviceProblem *d, const evp1d_fields *io, double rhow);
+// Rebuild the per-tile constant blocks from the slot arrays (after the
+// per-call fields or the drag factor changed).
+void problem_fill_const(DeviceProblem *d);
 // Results device -> host; waits for the stream.
 int problem_download(DeviceProblem *d, const evp1d_fields *io);
 

@@ -75,6 +75,12 @@ void launch_fused(const FusedArgs &a, const Params &p, bool last,
 // Tbu, uinit, vinit).
 constexpr int kTmaStressFields = 19;
 constexpr int kTmaStepuFields = 13;
+// Per-call constants of a tile in one contiguous block (one bulk copy per
+// tile instead of twenty): kConstFields x kTileOwned doubles per tile, fields
+// [0..5] dxT dyT HTE HTN HTEm1 HTNm1, [6] strength, [7..19] the 13 stepu
+// inputs in the uf order, [20] meta | lcor << 32; unused slots hold 0.
+constexpr int kConstFields = 21;
+constexpr int kConstTileSlots = 256;
 struct TmaArgs {
   int ntiles = 0;
   const int32_t *tile_off = nullptr, *tile_cnt = nullptr;
@@ -88,6 +94,7 @@ struct TmaArgs {
   const int32_t *tile_rec = nullptr;
   const double *sf[kTmaStressFields] = {};
   const double *uf[kTmaStepuFields] = {};
+  const double *cblk = nullptr;  // constant blocks, kConstFields x 256 per tile
   const double *u_in = nullptr, *v_in = nullptr;
   double *u_out = nullptr, *v_out = nullptr;
   double *s_out[12] = {};
@@ -126,6 +133,11 @@ void launch_gather(const PermBatch &b, int na, const int32_t *slot_of_point,
 void launch_flags(int nslots, const int32_t *point_of_slot,
                   const int32_t *skipT, const int32_t *skipU, uint8_t *flags,
                   const uint32_t *lnb, uint32_t *meta, cudaStream_t st);
+// cblk[(t*kConstFields + f)*256 + l] = src[f][tile_off[t] + l] for l <
+// tile_cnt[t] (f < 20), meta | lcor << 32 for f = 20, and 0 for l >= tile_cnt.
+void launch_const_blocks(int ntiles, const int32_t *tile_off, const int32_t *tile_cnt,
+                         const double *const src[kConstFields - 1], const uint32_t *meta,
+                         const uint32_t *lcor, double *cblk, cudaStream_t st);
 // kvrel[s] = (aiu[s]*rhow)*Cw[s].
 void launch_drag_factor(int nslots, const double *aiu, const double *Cw,
                         double rhow, double *kvrel, cudaStream_t st);

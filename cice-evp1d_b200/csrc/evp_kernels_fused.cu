@@ -201,4 +201,45 @@ void launch_drag_factor(int n, const double *aiu, const double *Cw,
   k_drag<<<blocks_for(n), 256, 0, st>>>(n, aiu, Cw, rhow, kv);
 }
 
+namespace {
+struct ConstSrc {
+  const double *f[kConstFields - 1];
+};
+
+__global__ void k_const_blocks(int ntiles, const int32_t *tile_off, const int32_t *tile_cnt,
+                               ConstSrc src, const uint32_t *meta, const uint32_t *lcor,
+                               double *cblk) {
+  const long long total = (long long)ntiles * kConstFields * kConstTileSlots;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int l = (int)(e % kConstTileSlots);
+    const long long tf = e / kConstTileSlots;
+    const int f = (int)(tf % kConstFields);
+    const int t = (int)(tf / kConstFields);
+    double v = 0.0;
+    if (l < tile_cnt[t]) {
+      const int s = tile_off[t] + l;
+      if (f < kConstFields - 1)
+        v = src.f[f][s];
+      else
+        v = __longlong_as_double((long long)((unsigned long long)meta[s] |
+                                             ((unsigned long long)lcor[s] << 32)));
+    }
+    cblk[e] = v;
+  }
+}
+}  // namespace
+
+void launch_const_blocks(int ntiles, const int32_t *tile_off, const int32_t *tile_cnt,
+                         const double *const src[kConstFields - 1], const uint32_t *meta,
+                         const uint32_t *lcor, double *cblk, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  ConstSrc cs;
+  for (int f = 0; f < kConstFields - 1; f++) cs.f[f] = src[f];
+  const long long total = (long long)ntiles * kConstFields * kConstTileSlots;
+  const long long b = (total + 255) / 256;
+  k_const_blocks<<<(int)(b < 148 * 32 ? b : 148 * 32), 256, 0, st>>>(ntiles, tile_off, tile_cnt,
+                                                                      cs, meta, lcor, cblk);
+}
+
 }  // namespace evp

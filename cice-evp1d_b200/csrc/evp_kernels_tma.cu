@@ -39,18 +39,19 @@ constexpr int kUV = kTileOwned + kTileUvx;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s
 
 struct Stage {
-  double sf[kTmaStressFields][kTileOwned];  // dxT..HTNm1, strength, 12 stresses
-  double uf[kTmaStepuFields][kTileOwned];   // stepu inputs
+  double cf[kConstFields][kTileOwned];  // the tile's constant block (one bulk copy)
+  double s12[12][kTileOwned];           // the 12 stresses
   double u[kUV];
   double v[kUV];
-  uint32_t meta[kTileOwned];
-  uint32_t lcor[kTileOwned];
-  double hf[kTmaStressFields][kTileHalo];
+  double hf[kTmaStressFields][kTileHalo];  // halo: 6 geometry, strength, 12 stresses
   uint32_t hmeta[kTileHalo];
   uint32_t hlcc[kTileHalo];
   uint32_t hlcor[kTileHalo];
   int hdr[4];  // tile offset, owned count, halo count (written by the producer)
 };
+
+static_assert(kConstTileSlots == kTileOwned, "constant blocks hold one tile");
+static_assert(kConstFields == 7 + kTmaStepuFields + 1, "constant block layout");
 
 struct Smem {
   Stage st[kStages];
@@ -235,27 +236,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       }
       __syncwarp();
       const uint32_t n4 = (uint32_t)((cnt + 3) & ~3);
-      const uint32_t b8 = n4 * 8u, b4 = n4 * 4u;
+      const uint32_t b8 = n4 * 8u;
+      constexpr uint32_t kConstBytes = kConstFields * kTileOwned * 8u;
       // release: the header and halo indices are visible to consumers once
       // the phase completes
-      if (lane == 0)
-        mbar_arrive_expect_tx(&S.full[s],
-                              (kTmaStressFields + kTmaStepuFields + 2) * b8 + 2 * b4);
+      if (lane == 0) mbar_arrive_expect_tx(&S.full[s], kConstBytes + 14 * b8);
       __syncwarp();
-      for (int k = lane; k < kTmaStressFields + kTmaStepuFields + 4; k += 32) {
-        if (k < kTmaStressFields)
-          bulk_g2s(st.sf[k], a.sf[k] + off, b8, &S.full[s]);
-        else if (k < kTmaStressFields + kTmaStepuFields)
-          bulk_g2s(st.uf[k - kTmaStressFields], a.uf[k - kTmaStressFields] + off, b8, &S.full[s]);
-        else if (k == kTmaStressFields + kTmaStepuFields)
-          bulk_g2s(st.u, a.u_in + off, b8, &S.full[s]);
-        else if (k == kTmaStressFields + kTmaStepuFields + 1)
-          bulk_g2s(st.v, a.v_in + off, b8, &S.full[s]);
-        else if (k == kTmaStressFields + kTmaStepuFields + 2)
-          bulk_g2s(st.meta, a.meta + off, b4, &S.full[s]);
-        else
-          bulk_g2s(st.lcor, a.lcor + off, b4, &S.full[s]);
-      }
+      if (lane == 0)
+        bulk_g2s(st.cf, a.cblk + (size_t)t * kConstFields * kTileOwned, kConstBytes, &S.full[s]);
+      else if (lane <= 12)
+        bulk_g2s(st.s12[lane - 1], a.sf[6 + lane] + off, b8, &S.full[s]);
+      else if (lane == 13)
+        bulk_g2s(st.u, a.u_in + off, b8, &S.full[s]);
+      else if (lane == 14)
+        bulk_g2s(st.v, a.v_in + off, b8, &S.full[s]);
       for (int x = lane; x < nx; x += 32) {
         const int g = rec[kRecUvx + x];
         cp_async8(&st.u[kTileOwned + x], a.u_in + g);
@@ -325,15 +319,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     const bool own = c < kTileOwned;
     const int h = c - kTileOwned;
     if (own ? c < cnt : h < nh) {
-      const uint32_t m = own ? st.meta[c] : st.hmeta[h];
+      uint32_t m, lc;
+      if (own) {
+        const unsigned long long ml = (unsigned long long)__double_as_longlong(st.cf[20][c]);
+        m = (uint32_t)ml;
+        lc = (uint32_t)(ml >> 32);
+      } else {
+        m = st.hmeta[h];
+        lc = st.hlcor[h];
+      }
       double out[8];
       if ((m >> 30) & kSkipT) {
 #pragma unroll
         for (int k = 0; k < 8; k++) out[k] = 0.0;
       } else {
-        const double *F = own ? &st.sf[0][c] : &st.hf[0][h];
+        // geometry and strength (fields 0..6), then the 12 stresses
+        const double *F = own ? &st.cf[0][c] : &st.hf[0][h];
+        const double *F12 = own ? &st.s12[0][c] : &st.hf[7][h];
         const int fs = own ? kTileOwned : kTileHalo;
-        const uint32_t lc = own ? st.lcor[c] : st.hlcor[h];
         const int cc = own ? c : (int)st.hlcc[h];
         const int iee = lc & kLnbMask, ine = (lc >> kLnbBits) & kLnbMask;
         const int ise = (lc >> (2 * kLnbBits)) & kLnbMask;
@@ -351,7 +354,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
         const Strain sr = strain_rates(cr, gm, p.e_factor);
         double s12[12];
 #pragma unroll
-        for (int k = 0; k < 12; k++) s12[k] = F[(7 + k) * fs];
+        for (int k = 0; k < 12; k++) s12[k] = F12[k * fs];
         stress_update(s12, out, sr, F[6 * fs], gm, p);
         if (own) {
 #pragma unroll
@@ -370,26 +373,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
 
     // ---------------- phase 2: stepu on owned points ------------------------
     if (c < cnt) {
-      const uint32_t m = st.meta[c];
+      const uint32_t m = (uint32_t)__double_as_longlong(st.cf[20][c]);
       if (!((m >> 30) & kSkipU)) {
         const int lnw = m & kLnbMask, lsw = (m >> kLnbBits) & kLnbMask;
         const int lsse = (m >> (2 * kLnbBits)) & kLnbMask;
         StepuIn in;
         in.uold = st.u[c];
         in.vold = st.v[c];
-        in.kvrel = st.uf[0][c];
-        in.uocn = st.uf[1][c];
-        in.vocn = st.uf[2][c];
-        in.waterx = st.uf[3][c];
-        in.watery = st.uf[4][c];
-        in.forcex = st.uf[5][c];
-        in.forcey = st.uf[6][c];
-        in.umassdti = st.uf[7][c];
-        in.fm = st.uf[8][c];
-        in.uarear = st.uf[9][c];
-        in.Tbu = st.uf[10][c];
-        in.uinit = st.uf[11][c];
-        in.vinit = st.uf[12][c];
+        in.kvrel = st.cf[7][c];
+        in.uocn = st.cf[8][c];
+        in.vocn = st.cf[9][c];
+        in.waterx = st.cf[10][c];
+        in.watery = st.cf[11][c];
+        in.forcex = st.cf[12][c];
+        in.forcey = st.cf[13][c];
+        in.umassdti = st.cf[14][c];
+        in.fm = st.cf[15][c];
+        in.uarear = st.cf[16][c];
+        in.Tbu = st.cf[17][c];
+        in.uinit = st.cf[18][c];
+        in.vinit = st.cf[19][c];
         in.s1 = S.str[0][c];
         in.s2nw = S.str[1][lnw];
         in.s3sse = S.str[2][lsse];

@@ -62,6 +62,7 @@ void layout(DeviceProblem *d, Carve &c, size_t nhalo_total, size_t nuvx_total) {
   c.take(&d->uvx_idx, nuvx_total);
   c.take(&d->tile_meta, 8 * T);
   c.take(&d->tile_rec, (size_t)kRecInts * T);
+  c.take(&d->cblk, (size_t)kConstFields * kConstTileSlots * T);
   c.take(&d->tile_off, T);
   c.take(&d->tile_cnt, T);
   c.take(&d->halo_off, T);
@@ -275,12 +276,24 @@ int problem_upload(DeviceProblem *d, const evp1d_fields *io, double rhow) {
     }
   }
   launch_drag_factor(d->nslots, d->dyn[kAiu], d->dyn[kCw], rhow, d->dyn[kKvrel], st);
+  problem_fill_const(d);
   for (int k = 0; k < 8; k++)
     CUDA_TRY(cudaMemsetAsync(d->str[k], 0, (size_t)d->nuv * sizeof(double), st));
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(st));
   d->cur = 0;
   return EVP1D_OK;
+}
+
+void problem_fill_const(DeviceProblem *d) {
+  if (d->ntiles == 0) return;
+  const double *src[kConstFields - 1] = {
+      d->geo[kDxT],  d->geo[kDyT],    d->geo[kHTE],    d->geo[kHTN],    d->geo[kHTEm1],
+      d->geo[kHTNm1], d->dyn[kStrength], d->dyn[kKvrel], d->dyn[kUocn], d->dyn[kVocn],
+      d->dyn[kWaterx], d->dyn[kWatery], d->dyn[kForcex], d->dyn[kForcey], d->dyn[kUmassdti],
+      d->dyn[kFm],   d->geo[kUarear], d->dyn[kTbu],    d->dyn[kUinit],  d->dyn[kVinit]};
+  launch_const_blocks(d->ntiles, d->tile_off, d->tile_cnt, src, d->meta, d->lcor, d->cblk,
+                      d->stream);
 }
 
 int problem_download(DeviceProblem *d, const evp1d_fields *io) {
@@ -449,6 +462,7 @@ TmaArgs problem_tma_args(const DeviceProblem &d, int from) {
                                          kTbu, kUinit, kVinit};
   for (int k = 0; k < kTmaStepuFields; k++)
     a.uf[k] = uf_order[k] < 0 ? d.geo[kUarear] : d.dyn[uf_order[k]];
+  a.cblk = d.cblk;
   a.u_in = d.u[from];
   a.v_in = d.v[from];
   a.u_out = d.u[to];
