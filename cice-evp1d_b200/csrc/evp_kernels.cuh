@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "evp_math.cuh"
+#include "evp_tiles.h"
 
 namespace evp {
 
@@ -80,7 +81,7 @@ constexpr int kTmaStepuFields = 13;
 // [0..5] dxT dyT HTE HTN HTEm1 HTNm1, [6] strength, [7..19] the 13 stepu
 // inputs in the uf order, [20] meta | lcor << 32; unused slots hold 0.
 constexpr int kConstFields = 21;
-constexpr int kConstTileSlots = 256;
+constexpr int kConstTileSlots = kTileOwned;
 struct TmaArgs {
   int ntiles = 0;
   const int32_t *tile_off = nullptr, *tile_cnt = nullptr;
@@ -94,7 +95,7 @@ struct TmaArgs {
   const int32_t *tile_rec = nullptr;
   const double *sf[kTmaStressFields] = {};
   const double *uf[kTmaStepuFields] = {};
-  const double *cblk = nullptr;  // constant blocks, kConstFields x 256 per tile
+  const double *cblk = nullptr;  // constant blocks, kConstFields x kTileOwned per tile
   const double *u_in = nullptr, *v_in = nullptr;
   double *u_out = nullptr, *v_out = nullptr;
   double *s_out[12] = {};

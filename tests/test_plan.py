@@ -9,6 +9,9 @@ from evp1d import synth
 import helpers
 
 
+TILE = 256  # kTileOwned (csrc/evp_tiles.h)
+
+
 def stats(pr):
     return evp1d.plan_stats(pr.na, pr.navel, pr.idx)
 
@@ -16,9 +19,9 @@ def stats(pr):
 def test_cfg1_plan_uses_full_compact_tiles():
     pr = synth.make_problem("cfg1")
     s = stats(pr)
-    # Hilbert-curve runs of 256 points: tiles nearly full, forward halo small
-    assert s["from_coords"] and s["max_halo"] <= 64 and s["max_tile"] <= 256
-    assert pr.na / s["tiles"] > 0.9 * 256
+    # Hilbert-curve runs of TILE points: tiles nearly full, forward halo small
+    assert s["from_coords"] and s["max_halo"] <= 64 and s["max_tile"] <= TILE
+    assert pr.na / s["tiles"] > 0.9 * TILE
     assert s["halo"] < 0.2 * s["slots"]
 
 
@@ -34,14 +37,14 @@ def test_shuffled_list_still_finds_grid():
 def test_random_graph_falls_back(na, nhalo, seed):
     pr = helpers.random_graph_problem(na, nhalo, seed)
     s = stats(pr)
-    assert s["max_halo"] <= 64 and s["max_tile"] <= 256
+    assert s["max_halo"] <= 64 and s["max_tile"] <= TILE
     if na > 10:
         assert not s["from_coords"]
 
 
 def test_standalone_plan():
     s = stats(helpers.standalone_problem())
-    # 441 points in runs of 256: two tiles
+    # 441 points in runs of TILE: two tiles
     assert s["from_coords"] and s["tiles"] == 2 and s["slots"] >= 441
 
 
