@@ -171,10 +171,49 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
       }
       return hkey[a] < hkey[b];
     });
-    for (int k = 0; k < na; k += kTileOwned) {
-      std::vector<int32_t> g(order.begin() + k,
-                             order.begin() + (k + kTileOwned < na ? k + kTileOwned : na));
-      groups.push_back(std::move(g));
+    // each tile takes the longest run (up to kTileOwned points) whose halo
+    // and velocity extras fit, found by bisection on the run length
+    std::vector<int32_t> m1((size_t)navel, -1), m2((size_t)navel, -1), m3((size_t)navel, -1);
+    int st = 0;
+    auto fits = [&](int k, int len) {
+      st++;
+      for (int q = k; q < k + len; q++) m1[order[q]] = st;
+      int nh = 0, nx = 0;
+      std::vector<int32_t> hl;
+      for (int q = k; q < k + len; q++)
+        for (int r = 3; r < 6; r++) {
+          const int n = nb0[r][order[q]];
+          if (n < na && m1[n] != st && m2[n] != st) {
+            m2[n] = st;
+            hl.push_back(n);
+            if (++nh > kTileHalo) return false;
+          }
+        }
+      auto add_x = [&](int n) {
+        if (m1[n] != st && m3[n] != st) {
+          m3[n] = st;
+          nx++;
+        }
+      };
+      for (int n : hl) add_x(n);
+      for (int q = k; q < k + len; q++)
+        for (int r = 0; r < 3; r++) add_x(nb0[r][order[q]]);
+      for (int n : hl)
+        for (int r = 0; r < 3; r++) add_x(nb0[r][n]);
+      return nx <= kTileUvx;
+    };
+    for (int k = 0; k < na;) {
+      int len = kTileOwned < na - k ? kTileOwned : na - k;
+      if (!fits(k, len)) {
+        int lo = 1, hi = len - 1;  // fits(k, 1) holds: a point reaches 3 + 6 + 9 others
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) / 2;
+          if (fits(k, mid)) lo = mid; else hi = mid - 1;
+        }
+        len = lo;
+      }
+      groups.emplace_back(order.begin() + k, order.begin() + k + len);
+      k += len;
     }
   } else {
     for (int k = 0; k < na; k += kTileOwned) {
