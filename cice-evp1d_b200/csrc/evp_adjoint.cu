@@ -68,6 +68,9 @@ struct AdjArgs {
   const uint8_t *flags = nullptr;
   const int32_t *ee = nullptr, *ne = nullptr, *se = nullptr;
   const int32_t *tr_off[kNumTr] = {}, *tr_idx[kNumTr] = {};
+  // when no list has more than one entry (grid-shaped problems): the entry or
+  // -1 per slot, read instead of the CSR lists
+  const int32_t *tr_one[kNumTr] = {};
   const double *dxT = nullptr, *dyT = nullptr, *HTE = nullptr, *HTN = nullptr;
   const double *HTEm1 = nullptr, *HTNm1 = nullptr, *uarear = nullptr;
   const double *strength = nullptr, *kvrel = nullptr, *aiu = nullptr;
@@ -82,29 +85,60 @@ struct AdjArgs {
 
 // lam of u(n+1), v(n+1) at x: stepu's own part plus the stress corners that
 // read the velocity at x (as cc of x, and as ee/ne/se of other T points).
+template <bool kOne>
 __device__ __forceinline__ void velocity_lam(const AdjArgs &a, int x, double &lu,
                                              double &lv) {
   lu = a.Pu[x] + a.C8[0][x];
   lv = a.Pv[x] + a.C8[1][x];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    const int32_t *off = a.tr_off[kTrEe + k], *idx = a.tr_idx[kTrEe + k];
-    const int b = off[x], e = off[x + 1];
-    for (int q = b; q < e; q++) {
-      const int w = idx[q];
-      lu += a.C8[2 + 2 * k][w];
-      lv += a.C8[3 + 2 * k][w];
+    if (kOne) {
+      const int w = a.tr_one[kTrEe + k][x];
+      if (w >= 0) {
+        lu += a.C8[2 + 2 * k][w];
+        lv += a.C8[3 + 2 * k][w];
+      }
+    } else {
+      const int32_t *off = a.tr_off[kTrEe + k], *idx = a.tr_idx[kTrEe + k];
+      const int b = off[x], e = off[x + 1];
+      for (int q = b; q < e; q++) {
+        const int w = idx[q];
+        lu += a.C8[2 + 2 * k][w];
+        lv += a.C8[3 + 2 * k][w];
+      }
     }
   }
 }
 
+// Sum of Lx and Ly over the U points of transposed list t at slot w.
+template <bool kOne>
+__device__ __forceinline__ void str_lam(const AdjArgs &a, int t, int w, double &sx,
+                                        double &sy) {
+  sx = 0.0;
+  sy = 0.0;
+  if (kOne) {
+    const int x = a.tr_one[t][w];
+    if (x >= 0) {
+      sx = a.Lx[x];
+      sy = a.Ly[x];
+    }
+  } else {
+    const int32_t *off = a.tr_off[t], *idx = a.tr_idx[t];
+    for (int q = off[w]; q < off[w + 1]; q++) {
+      sx += a.Lx[idx[q]];
+      sy += a.Ly[idx[q]];
+    }
+  }
+}
+
+template <bool kOne>
 __global__ void __launch_bounds__(kThreads)
 k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__restrict__ v0,
             const double *__restrict__ u1, const double *__restrict__ v1) {
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.nslots;
        x += gridDim.x * blockDim.x) {
     double lu, lv;
-    velocity_lam(a, x, lu, lv);
+    velocity_lam<kOne>(a, x, lu, lv);
     if (a.flags[x] & kSkipU) {  // u(n+1) = u(n) here
       a.Pu[x] = lu;
       a.Pv[x] = lv;
@@ -144,6 +178,7 @@ k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__
   }
 }
 
+template <bool kOne>
 __global__ void __launch_bounds__(kThreads, 2)
 k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__restrict__ v) {
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < a.nslots;
@@ -156,36 +191,9 @@ k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__
     double lo[8];
     lo[0] = a.Lx[w];
     lo[4] = a.Ly[w];
-    {
-      const int32_t *off = a.tr_off[kTrNw], *idx = a.tr_idx[kTrNw];
-      double sx = 0.0, sy = 0.0;
-      for (int q = off[w]; q < off[w + 1]; q++) {
-        sx += a.Lx[idx[q]];
-        sy += a.Ly[idx[q]];
-      }
-      lo[1] = sx;
-      lo[6] = sy;
-    }
-    {
-      const int32_t *off = a.tr_off[kTrSse], *idx = a.tr_idx[kTrSse];
-      double sx = 0.0, sy = 0.0;
-      for (int q = off[w]; q < off[w + 1]; q++) {
-        sx += a.Lx[idx[q]];
-        sy += a.Ly[idx[q]];
-      }
-      lo[2] = sx;
-      lo[5] = sy;
-    }
-    {
-      const int32_t *off = a.tr_off[kTrSw], *idx = a.tr_idx[kTrSw];
-      double sx = 0.0, sy = 0.0;
-      for (int q = off[w]; q < off[w + 1]; q++) {
-        sx += a.Lx[idx[q]];
-        sy += a.Ly[idx[q]];
-      }
-      lo[3] = sx;
-      lo[7] = sy;
-    }
+    str_lam<kOne>(a, kTrNw, w, lo[1], lo[6]);
+    str_lam<kOne>(a, kTrSse, w, lo[2], lo[5]);
+    str_lam<kOne>(a, kTrSw, w, lo[3], lo[7]);
     double ls[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) ls[k] = a.LS[k][w];
@@ -213,11 +221,12 @@ k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__
 
 // lam of the velocities at call start; fold_init adds the uvel_init part
 // when uvel_init was the call-start velocity.
+template <bool kOne>
 __global__ void __launch_bounds__(kThreads) k_adj_final(AdjArgs a, int fold_init) {
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.nslots;
        x += gridDim.x * blockDim.x) {
     double lu, lv;
-    velocity_lam(a, x, lu, lv);
+    velocity_lam<kOne>(a, x, lu, lv);
     if (fold_init) {
       lu += a.g[kGUinit][x];
       lv += a.g[kGVinit][x];
@@ -261,6 +270,8 @@ struct AdjointState {
   void *arena = nullptr;
   size_t arena_bytes = 0;
   int32_t *tr_off[kNumTr] = {}, *tr_idx[kNumTr] = {};
+  int32_t *tr_one[kNumTr] = {};
+  bool one = false;  // every transposed list has at most one entry
   double *Pu = nullptr, *Pv = nullptr, *Lx = nullptr, *Ly = nullptr;
   double *C8[8] = {}, *LS[12] = {}, *g[kNumGrad] = {};
   double *spp[2][12] = {};  // stress ping-pong of the segment recompute
@@ -337,9 +348,25 @@ int ensure_static(evp1d_t *h) {
       if (o >= 0 && o < S && pos[o] >= 0) idx[t][fill[o]++] = s;
     }
   }
+  // direct form when no list has two entries
+  bool one = true;
+  for (int t = 0; t < kNumTr && one; t++)
+    for (int w = 0; w < S; w++)
+      if (off[t][w + 1] - off[t][w] > 1) {
+        one = false;
+        break;
+      }
+  std::vector<int32_t> direct;
+  if (one) {
+    direct.assign((size_t)kNumTr * S, -1);
+    for (int t = 0; t < kNumTr; t++)
+      for (int w = 0; w < S; w++)
+        if (off[t][w + 1] > off[t][w]) direct[(size_t)t * S + w] = idx[t][off[t][w]];
+  }
+  A.one = one;
   // carve
   const size_t SD = pad256((size_t)S);
-  size_t ints = 0;
+  size_t ints = one ? (size_t)kNumTr * pad_ints((size_t)S) : 0;
   for (int t = 0; t < kNumTr; t++) ints += pad_ints(off[t].size()) + pad_ints(idx[t].size() + 1);
   const size_t ndbl = SD * (4 + 8 + 12 + kNumGrad + 24);
   A.arena_bytes = ints * sizeof(int32_t) + ndbl * sizeof(double);
@@ -365,6 +392,12 @@ int ensure_static(evp1d_t *h) {
     pi += pad_ints(off[t].size());
     A.tr_idx[t] = pi;
     pi += pad_ints(idx[t].size() + 1);
+    if (one) {
+      A.tr_one[t] = pi;
+      pi += pad_ints((size_t)S);
+      ADJ_TRY(cudaMemcpyAsync(A.tr_one[t], direct.data() + (size_t)t * S, sizeof(int32_t) * S,
+                              cudaMemcpyHostToDevice, st));
+    }
     ADJ_TRY(cudaMemcpyAsync(A.tr_off[t], off[t].data(), sizeof(int32_t) * off[t].size(),
                             cudaMemcpyHostToDevice, st));
     if (!idx[t].empty())
@@ -387,6 +420,7 @@ AdjArgs adj_args(const evp1d_t *h) {
   for (int t = 0; t < kNumTr; t++) {
     a.tr_off[t] = A.tr_off[t];
     a.tr_idx[t] = A.tr_idx[t];
+    a.tr_one[t] = A.tr_one[t];
   }
   a.dxT = d.geo[kDxT];
   a.dyT = d.geo[kDyT];
@@ -643,10 +677,16 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
   const AdjArgs a = adj_args(h);
   const int grid = blocks_for(d.nslots);
   long long launches = 0;
+  const bool one = A.one;
   auto reverse_step = [&](const double *u0, const double *v0, const double *u1,
                           const double *v1) {
-    k_adj_stepu<<<grid, kThreads, 0, st>>>(a, h->p, u0, v0, u1, v1);
-    k_adj_stress<<<grid, kThreads, 0, st>>>(a, h->p, u0, v0);
+    if (one) {
+      k_adj_stepu<true><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0, u1, v1);
+      k_adj_stress<true><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0);
+    } else {
+      k_adj_stepu<false><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0, u1, v1);
+      k_adj_stress<false><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0);
+    }
     launches += 2;
   };
   // taped tail
@@ -675,7 +715,10 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
     for (int i = len - 1; i >= 0; i--)
       reverse_step(tape_u(A, i), tape_v(A, i), tape_u(A, i + 1), tape_v(A, i + 1));
   }
-  k_adj_final<<<grid, kThreads, 0, st>>>(a, A.uinit_explicit ? 0 : 1);
+  if (one)
+    k_adj_final<true><<<grid, kThreads, 0, st>>>(a, A.uinit_explicit ? 0 : 1);
+  else
+    k_adj_final<false><<<grid, kThreads, 0, st>>>(a, A.uinit_explicit ? 0 : 1);
   launches++;
   ADJ_TRY(cudaGetLastError());
   A.launches = launches;

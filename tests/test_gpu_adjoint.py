@@ -290,3 +290,20 @@ def test_autograd_function_matches_tape(oracle_mod):
     t = evp_tape.gradient(pr, pr.ndte, evp1d.set_evp_parameters(pr.ndte), uobs, vobs, wrt=FIELDS)
     for k, x in zip(FIELDS, ins):
         assert rel(x.grad.numpy(), t[k]) < 1e-9, k
+
+
+@pytest.mark.parametrize("na,nhalo,seed", [(3000, 200, 4), (700, 9, 5)])
+def test_adjoint_irregular_graph_matches_tape(oracle_mod, na, nhalo, seed):
+    """Random (non-grid) neighbour vectors: points are read by several
+    neighbours, so the transposed lists have many entries (the general gather
+    path); gradients still match the tape."""
+    import evp_tape
+    import helpers
+    pr = helpers.random_graph_problem(na, nhalo, seed)
+    uobs, vobs = synth.observations(pr.na, seed=seed + 10)
+    g, _, _ = gpu_grads(pr, pr.ndte, uobs, vobs, interval=2, stress=True)
+    t = evp_tape.gradient(pr, pr.ndte, evp1d.set_evp_parameters(pr.ndte), uobs, vobs)
+    for k in FIELDS:
+        assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
+    assert rel(g["uvel"], t["uvel0"]) < 1e-9
+    assert rel(g["stress"], t["stress0"]) < 1e-9
