@@ -626,11 +626,14 @@ def main():
     peak, peak_src = alg_bytes.hbm_peak(ROOT)
 
     # ---------------- end to end (host buffers) ----------------
+    # inputs in page-locked host memory (evp1d_host_alloc), refilled with the
+    # step's starting state before each timed call
     h2d, d2h = alg_bytes.host_bytes(pr)
     e2e_times = []
+    fs_e = evp1d.FieldSet.from_problem(pr, pinned=True) if args.e2e_steps > 0 else None
     barrier()
     for _ in range(args.e2e_steps):
-        fs_e = evp1d.FieldSet.from_problem(pr)
+        fs_e.refill(pr)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -672,7 +675,8 @@ def main():
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_point_subcycle": ab,
                          "kernel": path},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e": {"value": e2e_value, "unit": UNIT, "host_memory": "page-locked",
+                    "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": sampler.summary() if sampler else None,

@@ -147,6 +147,18 @@ extern "C" {
 
 const char *evp1d_last_error(void) { return g_err.c_str(); }
 
+int evp1d_host_alloc(void **ptr, size_t bytes) {
+  if (!ptr) return fail(EVP1D_ERR_INVALID_ARG, "ptr is NULL");
+  *ptr = nullptr;
+  CUDA_TRY(cudaHostAlloc(ptr, bytes > 0 ? bytes : 1, cudaHostAllocPortable));
+  return EVP1D_OK;
+}
+
+int evp1d_host_free(void *ptr) {
+  if (ptr) CUDA_TRY(cudaFreeHost(ptr));
+  return EVP1D_OK;
+}
+
 const char *evp1d_version(void) {
   return "evp1d-b200 0.2 (sm_100a, fp64, fused tile solver)";
 }

@@ -15,6 +15,7 @@ only compute path.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -40,6 +41,27 @@ def set_evp_parameters(ndte: int) -> Params:
 
 def _d(a):
     return None if a is None else a.ctypes.data_as(_D)
+
+
+def pinned_empty(shape, dtype=np.float64) -> np.ndarray:
+    """A numpy array in page-locked host memory (evp1d_host_alloc), freed
+    when the array is garbage collected."""
+    L = _lib.load()
+    count = int(np.prod(shape))
+    nbytes = max(count * np.dtype(dtype).itemsize, 1)
+    p = C.c_void_p()
+    check(L.evp1d_host_alloc(C.byref(p), nbytes), "evp1d_host_alloc")
+    buf = (C.c_char * nbytes).from_address(p.value)
+    weakref.finalize(buf, L.evp1d_host_free, C.c_void_p(p.value))
+    return np.frombuffer(buf, dtype=dtype, count=count).reshape(shape)
+
+
+def pinned_copy(a) -> np.ndarray:
+    """A page-locked copy of `a`."""
+    a = np.asarray(a)
+    out = pinned_empty(a.shape, a.dtype)
+    out[...] = a
+    return out
 
 
 def _as_f64(a, n, name):
@@ -139,17 +161,35 @@ class FieldSet:
 
     @classmethod
     def from_problem(cls, prob, want_str: bool = False, copy: bool = True,
-                     explicit_init: bool = False) -> "FieldSet":
-        """Fields of a :class:`evp1d.synth.Problem1D` (copied by default)."""
-        cp = (lambda a: np.array(a, copy=True)) if copy else (lambda a: a)
+                     explicit_init: bool = False, pinned: bool = False) -> "FieldSet":
+        """Fields of a :class:`evp1d.synth.Problem1D` (copied by default;
+        into page-locked memory with ``pinned``)."""
+        if pinned:
+            cp = pinned_copy
+        else:
+            cp = (lambda a: np.array(a, copy=True)) if copy else (lambda a: a)
         dyn = {k: cp(prob.f[k]) for k in cls.DYN}
         return cls(prob.na, prob.navel, skipT=prob.skipT, skipU=prob.skipU,
                    stress=cp(prob.stress), uvel=cp(prob.uvel),
                    vvel=cp(prob.vvel), strintx=cp(prob.strintx),
                    strinty=cp(prob.strinty), Cb=cp(prob.Cb),
-                   uvel_init=prob.f["uvel_init"] if explicit_init else None,
-                   vvel_init=prob.f["vvel_init"] if explicit_init else None,
+                   uvel_init=cp(prob.f["uvel_init"]) if explicit_init else None,
+                   vvel_init=cp(prob.f["vvel_init"]) if explicit_init else None,
                    want_str=want_str, **dyn)
+
+    def refill(self, prob) -> None:
+        """Copy a problem's starting state and per-call fields into this
+        set's arrays (keeping their memory, e.g. page-locked)."""
+        self.stress[...] = prob.stress
+        self.uvel[...] = prob.uvel
+        self.vvel[...] = prob.vvel
+        self.strintx[...] = prob.strintx
+        self.strinty[...] = prob.strinty
+        self.Cb[...] = prob.Cb
+        self.skipT[...] = prob.skipT
+        self.skipU[...] = prob.skipU
+        for k in self.DYN:
+            self.dyn[k][...] = prob.f[k]
 
 
 class EVP1D:

@@ -120,6 +120,10 @@ def load() -> C.CDLL:
                  "evp1d_adjoint_seed", "evp1d_adjoint_sweep", "evp1d_adjoint_gradients",
                  "evp1d_adjoint_info", "evp1d_set_adjoint_budget"):
         getattr(L, name).restype = C.c_int
+    L.evp1d_host_alloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+    L.evp1d_host_alloc.restype = C.c_int
+    L.evp1d_host_free.argtypes = [C.c_void_p]
+    L.evp1d_host_free.restype = C.c_int
     L.evp1d_run_device_noalloc.argtypes = ([C.c_int, C.c_int] + [C.c_void_p] * 13
                                            + [C.POINTER(Params), C.c_int,
                                               C.POINTER(Fields), C.c_void_p])

@@ -26,6 +26,7 @@
 #ifndef EVP1D_H
 #define EVP1D_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -184,6 +185,15 @@ const char *evp1d_last_error(void);
 
 /* Library version string. */
 const char *evp1d_version(void);
+
+/* Page-locked (pinned) host memory for the arrays of evp1d_fields and
+ * evp1d_grads.  Copies from and to it run at full host-link speed and are
+ * asynchronous; pageable arrays work too, at lower speed.  A caller that keeps
+ * its fields in such memory across timesteps (as CICE keeps its module
+ * arrays) saves most of the transfer time of evp1d_run.  No counterpart in the
+ * reference. */
+int evp1d_host_alloc(void **ptr, size_t bytes);
+int evp1d_host_free(void *ptr);
 
 /* ----------------------------------------------------------------------------
  * Index build on the host, no GPU needed.

@@ -367,3 +367,21 @@ def test_sharded_run_single_rank_gpu(oracle_mod):
                                        vvel=st.vvel[: pr.navel], strintx=st.strintx,
                                        strinty=st.strinty, Cb=st.Cb), pr.na)
         assert got[i] == want
+
+
+def test_pinned_host_arrays_same_results(oracle_mod):
+    """Fields in page-locked host memory (evp1d_host_alloc) give the same bits
+    as pageable arrays, over two calls with a refill in between."""
+    pr = synth.make_problem("cfg1", nx=70, ny=55, ndte=9)
+    a = evp1d.FieldSet.from_problem(pr, want_str=False)
+    b = evp1d.FieldSet.from_problem(pr, want_str=False, pinned=True)
+    with evp1d.EVP1D.from_problem(pr) as s:
+        for _ in range(2):
+            s.run(pr.ndte, a)
+            s.run(pr.ndte, b)
+            for x, y in ((a.stress, b.stress), (a.uvel, b.uvel), (a.vvel, b.vvel),
+                         (a.strintx, b.strintx), (a.Cb, b.Cb)):
+                assert np.array_equal(x.view(np.int64), y.view(np.int64))
+        b.refill(pr)
+        s.run(pr.ndte, b)
+    assert_same(b, oracle_run(oracle_mod, pr, pr.ndte), pr, check_str=False)
