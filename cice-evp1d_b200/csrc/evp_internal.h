@@ -68,6 +68,15 @@ void problem_destroy(DeviceProblem *d);
 // uvel_init/vvel_init default to the uploaded velocities; the drag factor
 // (aiu*rhow)*Cw is precomputed; cur = 0.
 int problem_upload(DeviceProblem *d, const evp1d_fields *io, double rhow);
+// The device half of problem_upload: from the reference-order staging area
+// (slots 0..11 per-call inputs, 12..23 stresses, 24 u, 25 v [navel], 26 uinit,
+// 27 vinit, 28 strintx, 29 strinty, 30 Cb, 31 skipT then skipU as int32) into
+// the slot-ordered state.
+int problem_upload_staged(DeviceProblem *d, bool uinit_given, bool vinit_given, double rhow);
+// The device half of problem_download: slot-ordered results into the staging
+// area in reference order (slots 0..11 stresses, 12 u, 13 v, 14 strintx,
+// 15 strinty, 16 Cb, 17 + k str_k when want_str[k]).
+int problem_download_staged(DeviceProblem *d, const bool want_str[8]);
 // Rebuild the per-tile constant blocks from the slot arrays (after the
 // per-call fields or the drag factor changed).
 void problem_fill_const(DeviceProblem *d);

@@ -218,15 +218,8 @@ int problem_upload(DeviceProblem *d, const evp1d_fields *io, double rhow) {
   for (int k = 0; k < 12; k++) TRY(h2d(slot(12 + k), io->stress[k], bd, st));
   TRY(h2d(slot(24), io->uvel, bv, st));
   TRY(h2d(slot(25), io->vvel, bv, st));
-  const double *uinit_src = slot(24), *vinit_src = slot(25);
-  if (io->uvel_init) {
-    TRY(h2d(slot(26), io->uvel_init, bd, st));
-    uinit_src = slot(26);
-  }
-  if (io->vvel_init) {
-    TRY(h2d(slot(27), io->vvel_init, bd, st));
-    vinit_src = slot(27);
-  }
+  if (io->uvel_init) TRY(h2d(slot(26), io->uvel_init, bd, st));
+  if (io->vvel_init) TRY(h2d(slot(27), io->vvel_init, bd, st));
   TRY(h2d(slot(28), io->strintx, bd, st));
   TRY(h2d(slot(29), io->strinty, bd, st));
   TRY(h2d(slot(30), io->Cb, bd, st));
@@ -234,7 +227,18 @@ int problem_upload(DeviceProblem *d, const evp1d_fields *io, double rhow) {
   int32_t *skU = skT + navel;  // 2 x navel int32 fit in navel doubles
   TRY(h2d(skT, io->skipT, (size_t)na * sizeof(int32_t), st));
   TRY(h2d(skU, io->skipU, (size_t)na * sizeof(int32_t), st));
+  return problem_upload_staged(d, io->uvel_init != nullptr, io->vvel_init != nullptr, rhow);
+}
 
+int problem_upload_staged(DeviceProblem *d, bool uinit_given, bool vinit_given, double rhow) {
+  const int na = d->na, navel = d->navel;
+  if (na == 0) return EVP1D_OK;
+  cudaStream_t st = d->stream;
+  auto slot = [&](int k) { return d->stage + (size_t)k * navel; };
+  const double *uinit_src = uinit_given ? slot(26) : slot(24);
+  const double *vinit_src = vinit_given ? slot(27) : slot(25);
+  int32_t *skT = (int32_t *)slot(31);
+  int32_t *skU = skT + navel;
   launch_flags(d->nslots, d->point_of_slot, skT, skU, d->flags, d->lnb, d->meta, st);
   PermBatch a;  // single-copy fields
   for (int k = 0; k < 12; k++) {
@@ -301,6 +305,33 @@ int problem_download(DeviceProblem *d, const evp1d_fields *io) {
   if (na == 0) return EVP1D_OK;
   cudaStream_t st = d->stream;
   auto slot = [&](int k) { return d->stage + (size_t)k * navel; };
+  bool want_str[8];
+  for (int k = 0; k < 8; k++) want_str[k] = io->str[k] != nullptr;
+  TRY(problem_download_staged(d, want_str));
+  const size_t bd = (size_t)na * sizeof(double);
+  for (int k = 0; k < 12; k++)
+    if (io->stress[k]) TRY(d2h(io->stress[k], slot(k), bd, st));
+  if (io->uvel) TRY(d2h(io->uvel, slot(12), bd, st));
+  if (io->vvel) TRY(d2h(io->vvel, slot(13), bd, st));
+  if (io->strintx) TRY(d2h(io->strintx, slot(14), bd, st));
+  if (io->strinty) TRY(d2h(io->strinty, slot(15), bd, st));
+  if (io->Cb) TRY(d2h(io->Cb, slot(16), bd, st));
+  for (int k = 0; k < 8; k++)
+    if (io->str[k]) {
+      TRY(d2h(io->str[k], slot(17 + k), bd, st));
+      if (d->nhs > 0)
+        TRY(d2h(io->str[k] + na, d->str[k] + d->nslots,
+                (size_t)d->nhs * sizeof(double), st));
+    }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return EVP1D_OK;
+}
+
+int problem_download_staged(DeviceProblem *d, const bool want_str[8]) {
+  const int na = d->na, navel = d->navel;
+  if (na == 0) return EVP1D_OK;
+  cudaStream_t st = d->stream;
+  auto slot = [&](int k) { return d->stage + (size_t)k * navel; };
   PermBatch g;
   const int c = d->cur;
   for (int k = 0; k < 12; k++) {
@@ -318,28 +349,12 @@ int problem_download(DeviceProblem *d, const evp1d_fields *io) {
   g.src[g.n] = d->Cb;
   g.dst[g.n++] = slot(16);
   for (int k = 0; k < 8; k++)
-    if (io->str[k]) {
+    if (want_str[k]) {
       g.src[g.n] = d->str[k];
       g.dst[g.n++] = slot(17 + k);
     }
   launch_gather(g, na, d->slot_of_point, st);
   CUDA_TRY(cudaGetLastError());
-  const size_t bd = (size_t)na * sizeof(double);
-  for (int k = 0; k < 12; k++)
-    if (io->stress[k]) TRY(d2h(io->stress[k], slot(k), bd, st));
-  if (io->uvel) TRY(d2h(io->uvel, slot(12), bd, st));
-  if (io->vvel) TRY(d2h(io->vvel, slot(13), bd, st));
-  if (io->strintx) TRY(d2h(io->strintx, slot(14), bd, st));
-  if (io->strinty) TRY(d2h(io->strinty, slot(15), bd, st));
-  if (io->Cb) TRY(d2h(io->Cb, slot(16), bd, st));
-  for (int k = 0; k < 8; k++)
-    if (io->str[k]) {
-      TRY(d2h(io->str[k], slot(17 + k), bd, st));
-      if (d->nhs > 0)
-        TRY(d2h(io->str[k] + na, d->str[k] + d->nslots,
-                (size_t)d->nhs * sizeof(double), st));
-    }
-  CUDA_TRY(cudaStreamSynchronize(st));
   return EVP1D_OK;
 }
 

@@ -215,12 +215,14 @@ int evp1d_build_index(int nx, int ny, int nghost, const int32_t *mask,
  * 2D arrays (integration/ice_dyn_evp1d.F90:65-255, 326-331).  Arrays are
  * [nx*ny] column-major (i fastest) including the ghost cells, nx = nx_global
  * + 2*nghost as the adapter's G_* arrays (:93-94).  init builds the 1D list
- * from tmask (:559-589, 743-816); run derives skipT/skipU from the ice masks
- * (set_skipMe, :521-537), gathers the fields onto the list with halo
- * velocities 0 (convert_2d_1d_dyn, :818-882), runs ndte subcycles on the GPU
- * and scatters the results back (convert_1d_2d_dyn, :884-947).  Unlike the
- * reference, whose L_* arguments are intent(in), results are returned in the
- * inout arrays.
+ * from tmask (:559-589, 743-816); run copies the 2D arrays to the GPU, where
+ * kernels derive skipT/skipU from the ice masks (set_skipMe, :521-537),
+ * gather the fields onto the list with halo velocities 0 (convert_2d_1d_dyn,
+ * :818-882), run ndte subcycles and scatter the results back
+ * (convert_1d_2d_dyn, :884-947); the arrays come back whole, so cells outside
+ * the list keep the caller's values.  Unlike the reference, whose L_*
+ * arguments are intent(in), results are returned in the inout arrays.  With
+ * the arrays in evp1d_host_alloc memory the copies run at full speed.
  * -------------------------------------------------------------------------- */
 typedef struct evp1d_dyn_fields {
   double *stress[12];          /* inout: stressp_1..4, stressm_1..4, stress12_1..4 */

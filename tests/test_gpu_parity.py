@@ -354,6 +354,34 @@ def test_dyn2d_adapter_matches_v0(oracle_mod, curvilinear):
         assert np.array_equal(F[mine].view(np.int64), V[ref].view(np.int64)), mine
 
 
+def test_dyn2d_adapter_keeps_cells_outside_the_list(oracle_mod):
+    """Cells outside the 1D list (land) keep whatever the caller passed, and
+    a second call continues from the first call's state, as v0 does."""
+    from evp1d import dyn
+    g = synth.make_grid(48, 40, seed=19, ndte=6, curvilinear=True)
+    p = evp1d.set_evp_parameters(6)
+    F = dyn.fields_from_grid(g)
+    land = ~np.asarray(g.tmask, dtype=bool)
+    assert land.any()
+    marks = {k: np.float64(1234.5 + i) for i, k in enumerate(list(dyn.STRESS) + ["uvel", "vvel", "strintxU"])}
+    for k, v in marks.items():
+        F[k][land] = v
+    with dyn.Dyn2D(g.tmask, g.f["dyT"], g.f["dxT"], g.f["uarear"], g.f["HTE"],
+                   g.f["HTN"], p) as d:
+        d.run(6, F, g.iceT, g.iceU)
+        d.run(6, F, g.iceT, g.iceU)
+    for k, v in marks.items():
+        assert np.all(F[k][land] == v), k
+    G = dyn.fields_from_grid(g)
+    with dyn.Dyn2D(g.tmask, g.f["dyT"], g.f["dxT"], g.f["uarear"], g.f["HTE"],
+                   g.f["HTN"], p) as d:
+        d.run(6, G, g.iceT, g.iceU)
+        d.run(6, G, g.iceT, g.iceU)
+    sea = ~land
+    for k in list(dyn.STRESS) + ["uvel", "vvel", "strintxU", "strintyU", "Cb"]:
+        assert np.array_equal(F[k][sea].view(np.int64), G[k][sea].view(np.int64)), k
+
+
 def test_sharded_run_single_rank_gpu(oracle_mod):
     """The ensemble driver on one rank (no process group) solves its members
     on the GPU with the same summaries as the oracle."""
