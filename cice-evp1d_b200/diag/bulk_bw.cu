@@ -125,6 +125,8 @@ int main() {
       {18, 2048, 2}, {18, 2048, 4}, {18, 2048, 6},     // half tiles, more stages
       {36, 1024, 2}, {36, 1024, 4}, {36, 1024, 5},     // 128-point tiles
       {36, 2048, -1}, {36, 2048, -2}, {1, 73728, -1},  // from L2
+      {1, 73728, 1}, {2, 36864, 1}, {4, 18432, 1},      // one tile in flight, fewer copies
+      {15, 4096, 1}, {9, 8192, 1},
   };
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
