@@ -10,7 +10,12 @@ import ctypes as C
 import os
 
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_ROOT, "lib", "libevp1d.so")
+# EVP1D_LIBRARY=fma selects the FMA flavour (lib/libevp1d_fma.so); any other
+# value is a path to a build of the library.
+_FLAVOUR = os.environ.get("EVP1D_LIBRARY", "")
+FLAVOUR = "fma" if _FLAVOUR == "fma" else ("exact" if not _FLAVOUR else "custom")
+LIB_PATH = (os.path.join(PKG_ROOT, "lib", "libevp1d_fma.so") if _FLAVOUR == "fma"
+            else _FLAVOUR or os.path.join(PKG_ROOT, "lib", "libevp1d.so"))
 
 EVP1D_OK = 0
 ERRORS = {
