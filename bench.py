@@ -625,6 +625,36 @@ def main():
     achieved = ab * pr.n_active / sub_s / 1e9
     peak, peak_src = alg_bytes.hbm_peak(ROOT)
 
+    # ---------------- lindividual: stress alone, stepu alone ----------------
+    # the reference-order kernels of the lindividual loops (src/evp_v2b.F90:
+    # 127-155), timed on the device-resident state
+    n_ind = min(ndte, 200)
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1000.0
+
+    solver.stress_only(2)
+    solver.stepu_only(2)
+    t_so = timed(lambda: solver.stress_only(n_ind))
+    t_uo = timed(lambda: solver.stepu_only(n_ind))
+    # algorithmic bytes per point: stress reads 7 inputs, 12 stresses and the
+    # point's u, v, writes 12 stresses and 8 str, plus 3 indices and a flag;
+    # stepu reads 14 inputs, u, v and 8 str, writes u, v, strintx, strinty,
+    # Cb, plus 3 indices and a flag
+    b_so, b_uo = 41 * 8 + 13, 29 * 8 + 13
+    lind = {"subcycles": n_ind,
+            "stress_only": pr.n_active * n_ind / t_so,
+            "stepu_only": pr.n_active * n_ind / t_uo,
+            "stress_bytes_per_point": b_so, "stepu_bytes_per_point": b_uo,
+            "stress_frac": b_so * pr.n_active * n_ind / t_so / 1e9 / alg_bytes.hbm_peak(ROOT)[0],
+            "stepu_frac": b_uo * pr.n_active * n_ind / t_uo / 1e9 / alg_bytes.hbm_peak(ROOT)[0]}
+
     # ---------------- end to end (host buffers) ----------------
     # inputs in page-locked host memory (evp1d_host_alloc), refilled with the
     # step's starting state before each timed call
@@ -680,6 +710,7 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": sampler.summary() if sampler else None,
+            "lindividual": lind,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

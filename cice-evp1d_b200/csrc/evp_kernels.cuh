@@ -104,8 +104,8 @@ struct TmaArgs {
   int *err = nullptr;  // nonzero after a bounded wait ran out
   int prefetch = 0;    // tiles prefetched into L2 ahead of the shared ring
   // optional timing trace of block 0 (debug): per tile 8 %globaltimer stamps
-  // [0] producer issued, [1] A got the stage, [2] A corners done, [3] A str
-  // done, [4] B got the stage, [5] B done; kTraceTiles tiles at most
+  // [0] producer issued, [1] consumers have the stage, [2] stress done,
+  // [5] stepu done (3, 4, 6, 7 unused); kTraceTiles tiles at most
   long long *trace = nullptr;
 };
 constexpr int kTraceTiles = 256;

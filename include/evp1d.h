@@ -164,8 +164,9 @@ int evp1d_synchronize(evp1d_t *handle);
 
 /* Debug: timing trace of the TMA kernel's block 0 in the last launch
  * (recorded only when EVP1D_TRACE is set at evp1d_init).  Up to 256 tiles x 8
- * %globaltimer stamps (ns): producer issued, group A got the stage, corners
- * done, str done, group B got the stage, stepu done, 2 unused. */
+ * %globaltimer stamps (ns): [0] producer issued the tile's copies, [1] the
+ * consumers have the stage, [2] stress done, [5] stepu done; 3, 4, 6, 7
+ * unused (0). */
 int evp1d_debug_trace(evp1d_t *handle, long long *out, int n);
 
 /* Name of the subcycle kernel the handle runs: "fused-tile-tma" (default,
