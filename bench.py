@@ -35,6 +35,11 @@ for _p in (os.path.join(ROOT, "cice-evp1d_b200"), os.path.join(ROOT, "oracle")):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
+# the CPU baseline's OpenMP threads stay on their cores (read by libgomp when
+# the oracle library is first loaded)
+os.environ.setdefault("OMP_PROC_BIND", "close")
+os.environ.setdefault("OMP_PLACES", "cores")
+
 METRIC = "EVP ice-point-subcycles/s (FP64)"
 UNIT = "ice-point-subcycles/s"
 
@@ -687,7 +692,13 @@ def main():
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{pr.n_active} points x {n_sub} subcycles ({secs:.1f} s), "
                          f"oracle OpenMP SPMD port of src/evp_v2b.F90:91-110, f1 flags, "
-                         f"{threads} threads, {cpu_model()}"}
+                         f"{threads} threads, OMP_PROC_BIND={os.environ.get('OMP_PROC_BIND')}, "
+                         f"{cpu_model()}"}
+        # the same loop built for speed (the reference's f2-like flags:
+        # -O3 -march=x86-64-v3, FMA contraction allowed), for context
+        rate2, _, n2, secs2 = cpu_rate(pr, ndte, args.cpu_seconds / 2, flavour="f2")
+        cpu["f2"] = {"value": rate2, "flags": "-O3 -march=x86-64-v3 -fopenmp",
+                     "sample": f"{pr.n_active} points x {n2} subcycles ({secs2:.1f} s)"}
 
     path = solver.path
     solver.finalize()
