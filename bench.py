@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--config", default="cfg2")
+    ap.add_argument("--config", default="grid1600x1200")
     ap.add_argument("--ndte", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
@@ -553,10 +553,10 @@ def main():
         run_reference(args, rank, world)
         return
     from evp1d import synth as _synth
-    if args.config == "cfg4":
+    if args.config == "adjoint800x600":
         run_adjoint(args, rank, world, local)
         return
-    if args.config == "cfg5":
+    if args.config == "adjoint_ens32":
         run_adjoint_batched(args, rank, world, local)
         return
     if args.config in _synth.ENSEMBLES:

@@ -200,7 +200,7 @@ int check_device(int device) {
   cudaDeviceProp prop;
   CUDA_TRY(cudaGetDeviceProperties(&prop, device));
   if (prop.major != 10)
-    return fail(EVP1D_ERR_NO_DEVICE, "device %d is sm_%d%d; this build needs sm_100a",
+    return fail(EVP1D_ERR_NO_DEVICE, "device %d is sm_%d%d; the library is compiled for sm_100a",
                 device, prop.major, prop.minor);
   return EVP1D_OK;
 }

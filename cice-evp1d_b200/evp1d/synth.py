@@ -278,10 +278,10 @@ def to_1d(grid: Grid2D) -> Problem1D:
 
 # Benchmark configurations (shapes of the reference's evaluation cases).
 CONFIGS = {
-    "cfg1": dict(nx=400, ny=300, seed=1, ndte=120),
-    "cfg2": dict(nx=1600, ny=1200, seed=2, ndte=1000),
+    "grid400x300": dict(nx=400, ny=300, seed=1, ndte=120),
+    "grid1600x1200": dict(nx=1600, ny=1200, seed=2, ndte=1000),
     # adjoint workload: 800 x 600, ndte = 500, checkpoints every 50 subcycles
-    "cfg4": dict(nx=800, ny=600, seed=4, ndte=500),
+    "adjoint800x600": dict(nx=800, ny=600, seed=4, ndte=500),
 }
 
 ADJOINT_INTERVAL = 50
@@ -294,7 +294,7 @@ def observations(na: int, seed: int) -> tuple:
     return rng.normal(0.0, 0.1, na), rng.normal(0.0, 0.1, na)
 
 
-def make_problem(name: str = "cfg1", **over) -> Problem1D:
+def make_problem(name: str = "grid400x300", **over) -> Problem1D:
     kw = dict(CONFIGS[name])
     kw.update(over)
     return to_1d(make_grid(**kw))
@@ -356,7 +356,7 @@ def concat(members: list) -> Ensemble:
 
 # Ensemble configurations (uneven member domains).
 ENSEMBLES = {
-    "cfg3": dict(n_members=64, ny=300, nx_lo=100, nx_hi=1300, seed=3, ndte=500),
+    "ens64": dict(n_members=64, ny=300, nx_lo=100, nx_hi=1300, seed=3, ndte=500),
     # batched adjoint: gradients of the misfit with respect to forcex, forcey
-    "cfg5": dict(n_members=32, ny=600, nx_lo=300, nx_hi=1300, seed=5, ndte=1000),
+    "adjoint_ens32": dict(n_members=32, ny=600, nx_lo=300, nx_hi=1300, seed=5, ndte=1000),
 }

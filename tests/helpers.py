@@ -109,7 +109,7 @@ def random_graph_problem(na: int, nhalo: int, seed: int) -> synth.Problem1D:
     exists, which exercises the consecutive-point tiling and halo splitting."""
     rng = np.random.default_rng(seed)
     navel = na + nhalo
-    base = synth.make_problem("cfg1", nx=60, ny=50, seed=seed, ndte=5)
+    base = synth.make_problem("grid400x300", nx=60, ny=50, seed=seed, ndte=5)
     reps = -(-na // base.na)
     f = {k: np.tile(v, reps)[:na].copy() for k, v in base.f.items()}
     idx = {k: rng.integers(1, navel + 1, na).astype(np.int32)

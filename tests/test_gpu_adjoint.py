@@ -152,10 +152,10 @@ def central_difference(run, pr, field, d, h, uobs, vobs):
 
 
 def test_adjoint_matches_finite_differences():
-    """cfg1-sized grid (400 x 300), ndte = 120: directional derivatives of J
+    """grid400x300-sized grid (400 x 300), ndte = 120: directional derivatives of J
     along 8 random directions per field against central differences of the
     GPU forward, step 1e-6 relative."""
-    pr = synth.make_problem("cfg1")
+    pr = synth.make_problem("grid400x300")
     ndte = pr.ndte
     uobs, vobs = synth.observations(pr.na, seed=404)
     g, fs0, _ = gpu_grads(pr, ndte, uobs, vobs, interval=synth.ADJOINT_INTERVAL)

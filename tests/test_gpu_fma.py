@@ -1,7 +1,7 @@
 """GPU test of the FMA flavour (lib/libevp1d_fma.so, EVP1D_LIBRARY=fma): the
 same solver with a*b+c contracted into fused multiply-adds agrees with the
 bit-exact oracle to <= 1e-12 relative (max-norm over each output field, each
-field stated separately), on cfg1 (ndte = 120) and on a small grid run for
+field stated separately), on grid400x300 (ndte = 120) and on a small grid run for
 1000 subcycles."""
 import os
 import subprocess
@@ -24,7 +24,7 @@ import evp1d
 from evp1d import synth, _lib
 assert _lib.FLAVOUR == "fma"
 name, out = sys.argv[2], sys.argv[3]
-pr = synth.make_problem("cfg1") if name == "cfg1" else \
+pr = synth.make_problem("grid400x300") if name == "grid400x300" else \
     synth.to_1d(synth.make_grid(90, 70, seed=61, ndte=1000, curvilinear=True))
 fs = evp1d.FieldSet.from_problem(pr)
 with evp1d.EVP1D.from_problem(pr) as s:
@@ -34,7 +34,7 @@ np.savez(out, stress=fs.stress, uvel=fs.uvel[:pr.na], vvel=fs.vvel[:pr.na],
 """
 
 
-@pytest.mark.parametrize("case", ["cfg1", "long"])
+@pytest.mark.parametrize("case", ["grid400x300", "long"])
 def test_fma_flavour_within_1e12(oracle_mod, case, tmp_path):
     lib = os.path.join(PKG, "lib", "libevp1d_fma.so")
     if not os.path.exists(lib):
@@ -43,7 +43,7 @@ def test_fma_flavour_within_1e12(oracle_mod, case, tmp_path):
     env = dict(os.environ, EVP1D_LIBRARY="fma")
     subprocess.run([sys.executable, "-c", CHILD, PKG, case, out], check=True, env=env)
     got = np.load(out)
-    pr = synth.make_problem("cfg1") if case == "cfg1" else \
+    pr = synth.make_problem("grid400x300") if case == "grid400x300" else \
         synth.to_1d(synth.make_grid(90, 70, seed=61, ndte=1000, curvilinear=True))
     st = oracle_mod.run_1d(pr, pr.ndte)
     ref = dict(stress=st.stress, uvel=st.uvel[: pr.na], vvel=st.vvel[: pr.na],

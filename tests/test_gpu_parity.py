@@ -54,9 +54,9 @@ def test_small_grids_bitwise(oracle_mod, nx, ny, seed, ndte, curvilinear):
     assert_same(gpu_run(pr, ndte), oracle_run(oracle_mod, pr, ndte), pr)
 
 
-def test_cfg1_full_md5(oracle_mod):
+def test_grid400x300_full_md5(oracle_mod):
     """400 x 300 synthetic grid, ndte = 120: md5-identical output files."""
-    pr = synth.make_problem("cfg1")
+    pr = synth.make_problem("grid400x300")
     assert_same(gpu_run(pr, pr.ndte, want_str=False), oracle_run(oracle_mod, pr, pr.ndte),
                 pr, check_str=False)
 
@@ -64,7 +64,7 @@ def test_cfg1_full_md5(oracle_mod):
 def test_two_calls_carry_state(oracle_mod):
     """Two dyn_evp1d_run calls in a row: the second starts from the first's
     stresses and velocities."""
-    pr = synth.make_problem("cfg1", nx=80, ny=60, ndte=10)
+    pr = synth.make_problem("grid400x300", nx=80, ny=60, ndte=10)
     fs = gpu_run(pr, 10, calls=2)
     st = oracle_run(oracle_mod, pr, 10)
     pr2 = pr.copy()
@@ -117,7 +117,7 @@ def test_every_parameter_path(oracle_mod):
 def test_halo_velocity_read_as_given(oracle_mod):
     """Halo slots of uvel/vvel are inputs (src/vars.F90:2108 reads
     uvel(1:navel)); nonzero halo values feed the stress gathers."""
-    pr = synth.make_problem("cfg1", nx=50, ny=40, ndte=6)
+    pr = synth.make_problem("grid400x300", nx=50, ny=40, ndte=6)
     rng = np.random.default_rng(2)
     pr.uvel[pr.na:] = rng.normal(0, 0.05, pr.navel - pr.na)
     pr.vvel[pr.na:] = rng.normal(0, 0.05, pr.navel - pr.na)
@@ -128,7 +128,7 @@ def test_halo_velocity_read_as_given(oracle_mod):
 
 @pytest.mark.parametrize("which", ["allT", "allU", "none"])
 def test_skip_patterns(oracle_mod, which):
-    pr = synth.make_problem("cfg1", nx=40, ny=30, ndte=5)
+    pr = synth.make_problem("grid400x300", nx=40, ny=30, ndte=5)
     if which == "allT":
         pr.skipT[:] = 1
     elif which == "allU":
@@ -155,7 +155,7 @@ def test_empty_problem():
 
 def test_lindividual_loops(oracle_mod):
     """stress alone n times, then stepu alone n times (src/evp_v2b.F90:127-155)."""
-    pr = synth.make_problem("cfg1", nx=60, ny=45, ndte=4)
+    pr = synth.make_problem("grid400x300", nx=60, ny=45, ndte=4)
     fs = evp1d.FieldSet.from_problem(pr, want_str=True)
     st = oracle_mod.State1D(pr)
     op = oracle_mod.params(4)
@@ -170,7 +170,7 @@ def test_lindividual_loops(oracle_mod):
 
 
 def test_error_paths_on_device():
-    pr = synth.make_problem("cfg1", nx=30, ny=20, ndte=3)
+    pr = synth.make_problem("grid400x300", nx=30, ny=20, ndte=3)
     with evp1d.EVP1D.from_problem(pr, ndte=3) as s:
         with pytest.raises(evp1d.EVP1DError) as e:
             s.subcycles(3)  # nothing uploaded
@@ -189,7 +189,7 @@ def test_error_paths_on_device():
 
 
 def test_launch_count_is_native():
-    pr = synth.make_problem("cfg1", nx=30, ny=20, ndte=7)
+    pr = synth.make_problem("grid400x300", nx=30, ny=20, ndte=7)
     fs = evp1d.FieldSet.from_problem(pr)
     with evp1d.EVP1D.from_problem(pr, ndte=7) as s:
         s.launch_count(reset=True)
@@ -200,7 +200,7 @@ def test_launch_count_is_native():
 def test_shuffled_list_order(oracle_mod):
     """A list in random order: the solver rebuilds the grid tiles from the
     neighbour graph; results stay bitwise equal."""
-    pr = helpers.shuffle_problem(synth.make_problem("cfg1", nx=90, ny=70, ndte=9), 7)
+    pr = helpers.shuffle_problem(synth.make_problem("grid400x300", nx=90, ny=70, ndte=9), 7)
     assert_same(gpu_run(pr, 9), oracle_run(oracle_mod, pr, 9), pr)
 
 
@@ -216,7 +216,7 @@ def test_irregular_graph(oracle_mod, na, nhalo, seed):
 def test_graph_chunk_boundaries(oracle_mod, ndte):
     """Subcycle counts around the captured-graph chunk (50) and both
     ping-pong parities."""
-    pr = synth.make_problem("cfg1", nx=40, ny=30, ndte=ndte)
+    pr = synth.make_problem("grid400x300", nx=40, ny=30, ndte=ndte)
     assert_same(gpu_run(pr, ndte), oracle_run(oracle_mod, pr, ndte), pr)
 
 
@@ -228,7 +228,7 @@ def test_kernel_paths(oracle_mod, monkeypatch, path):
         monkeypatch.setenv("EVP1D_PATH", "fused")
     else:
         monkeypatch.delenv("EVP1D_PATH", raising=False)
-    pr = synth.make_problem("cfg1", nx=150, ny=110, ndte=11)
+    pr = synth.make_problem("grid400x300", nx=150, ny=110, ndte=11)
     fs = evp1d.FieldSet.from_problem(pr, want_str=True)
     with evp1d.EVP1D.from_problem(pr, ndte=11) as s:
         assert s.path == ("fused-tile" if path == "fused" else "fused-tile-tma")
@@ -256,7 +256,7 @@ def test_shortcut_edges(oracle_mod, u0):
     """Inputs at the edges of the solver's exact shortcuts: signed zeros in
     Tbu and fm, negative drag factors, zero strength, zero cell area (no
     Delta floor), resting ice with u0 = 0 (0/0 in Cb)."""
-    pr = synth.make_problem("cfg1", nx=60, ny=44, seed=13, ndte=7)
+    pr = synth.make_problem("grid400x300", nx=60, ny=44, seed=13, ndte=7)
     rng = np.random.default_rng(9)
     n = pr.na
     pick = lambda f: rng.random(n) < f
@@ -289,7 +289,7 @@ def test_golden_fixture_md5():
 def test_batched_ensemble_matches_members(oracle_mod):
     """Uneven members solved in one handle give, member by member, bitwise the
     single-member results (and the oracle's)."""
-    members = [synth.make_problem("cfg1", nx=nx, ny=ny, seed=40 + i, ndte=8)
+    members = [synth.make_problem("grid400x300", nx=nx, ny=ny, seed=40 + i, ndte=8)
                for i, (nx, ny) in enumerate([(30, 20), (75, 41), (12, 9), (50, 60), (90, 17)])]
     ens = synth.concat(members)
     fs = evp1d.FieldSet.from_problem(ens.combined, want_str=True)
@@ -308,7 +308,7 @@ def test_batched_ensemble_matches_members(oracle_mod):
 
 
 def test_autotune_keeps_state(oracle_mod):
-    pr = synth.make_problem("cfg1", nx=120, ny=90, ndte=12)
+    pr = synth.make_problem("grid400x300", nx=120, ny=90, ndte=12)
     fs = evp1d.FieldSet.from_problem(pr, want_str=True)
     with evp1d.EVP1D.from_problem(pr, ndte=12) as s:
         s.upload(fs)
@@ -386,7 +386,7 @@ def test_sharded_run_single_rank_gpu(oracle_mod):
     """The ensemble driver on one rank (no process group) solves its members
     on the GPU with the same summaries as the oracle."""
     from evp1d import ensemble
-    members = [synth.make_problem("cfg1", nx=nx, ny=25, seed=90 + i, ndte=5)
+    members = [synth.make_problem("grid400x300", nx=nx, ny=25, seed=90 + i, ndte=5)
                for i, nx in enumerate([20, 47, 33])]
     got = ensemble.sharded_run(members, 5)
     for i, pr in enumerate(members):
@@ -400,7 +400,7 @@ def test_sharded_run_single_rank_gpu(oracle_mod):
 def test_pinned_host_arrays_same_results(oracle_mod):
     """Fields in page-locked host memory (evp1d_host_alloc) give the same bits
     as pageable arrays, over two calls with a refill in between."""
-    pr = synth.make_problem("cfg1", nx=70, ny=55, ndte=9)
+    pr = synth.make_problem("grid400x300", nx=70, ny=55, ndte=9)
     a = evp1d.FieldSet.from_problem(pr, want_str=False)
     b = evp1d.FieldSet.from_problem(pr, want_str=False, pinned=True)
     with evp1d.EVP1D.from_problem(pr) as s:

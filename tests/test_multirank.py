@@ -30,7 +30,7 @@ def _oracle_solve(members, ndte):
 
 def _members():
     from evp1d import synth
-    return [synth.make_problem("cfg1", nx=nx, ny=30, seed=70 + i, ndte=4)
+    return [synth.make_problem("grid400x300", nx=nx, ny=30, seed=70 + i, ndte=4)
             for i, nx in enumerate([25, 60, 12, 44, 33])]
 
 

@@ -26,10 +26,10 @@ def test_v0_equals_v2_md5(oracle_mod, nx, ny, seed, ndte, curvilinear):
     assert not np.array_equal(st.uvel[: pr.na], pr.uvel[: pr.na])
 
 
-def test_v0_equals_v2_cfg1_short(oracle_mod):
+def test_v0_equals_v2_grid400x300_short(oracle_mod):
     """The 400 x 300 configuration, 3 subcycles (the full 120 run lives in the
     GPU parity tests)."""
-    g = synth.make_grid(**synth.CONFIGS["cfg1"])
+    g = synth.make_grid(**synth.CONFIGS["grid400x300"])
     pr = synth.to_1d(g)
     assert 40_000 < pr.na < 120_000
     st = oracle_mod.run_1d(pr, 3, p=oracle_mod.params(pr.ndte))
@@ -41,7 +41,7 @@ def test_v0_equals_v2_cfg1_short(oracle_mod):
 
 @pytest.mark.parametrize("nthreads", [2, 3, 8])
 def test_omp_spmd_equals_serial(oracle_mod, nthreads):
-    pr = synth.make_problem("cfg1", nx=120, ny=90, ndte=9)
+    pr = synth.make_problem("grid400x300", nx=120, ny=90, ndte=9)
     a = oracle_mod.run_1d(pr, 9)
     b = oracle_mod.run_1d(pr, 9, mode="omp", nthreads=nthreads)
     for k in ("stress", "uvel", "vvel", "strintx", "strinty", "Cb", "str"):
@@ -66,7 +66,7 @@ def test_omp_domain_split(oracle_mod):
 
 def test_stress_only_then_stepu_only(oracle_mod):
     """lindividual loops (src/evp_v2b.F90:127-155) compose to one subcycle."""
-    pr = synth.make_problem("cfg1", nx=50, ny=40, ndte=5)
+    pr = synth.make_problem("grid400x300", nx=50, ny=40, ndte=5)
     a = oracle_mod.run_1d(pr, 1, p=oracle_mod.params(5))
     st = oracle_mod.State1D(pr)
     oracle_mod.run_1d(pr, 1, p=oracle_mod.params(5), mode="stress", state=st)

@@ -16,8 +16,8 @@ def stats(pr):
     return evp1d.plan_stats(pr.na, pr.navel, pr.idx)
 
 
-def test_cfg1_plan_uses_full_compact_tiles():
-    pr = synth.make_problem("cfg1")
+def test_grid400x300_plan_uses_full_compact_tiles():
+    pr = synth.make_problem("grid400x300")
     s = stats(pr)
     # Hilbert-curve runs of TILE points: tiles nearly full, forward halo small
     assert s["from_coords"] and s["max_halo"] <= 64 and s["max_tile"] <= TILE
@@ -26,7 +26,7 @@ def test_cfg1_plan_uses_full_compact_tiles():
 
 
 def test_shuffled_list_still_finds_grid():
-    pr = synth.make_problem("cfg1", nx=90, ny=70)
+    pr = synth.make_problem("grid400x300", nx=90, ny=70)
     a = stats(pr)
     b = stats(helpers.shuffle_problem(pr, 4))
     assert b["from_coords"]

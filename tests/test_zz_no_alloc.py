@@ -94,7 +94,7 @@ def _assert_same(dev, fs, check_str=True):
 
 @pytest.mark.parametrize("explicit_init", [False, True])
 def test_two_calls_match_evp1d_run(explicit_init):
-    pr = synth.make_problem("cfg1", nx=150, ny=110, ndte=17)
+    pr = synth.make_problem("grid400x300", nx=150, ny=110, ndte=17)
     assert pr.navel <= MAX_NAVEL
     ndte = pr.ndte
     params = evp1d.set_evp_parameters(ndte)
@@ -111,7 +111,7 @@ def test_two_calls_match_evp1d_run(explicit_init):
 
 def test_other_sizes_between_calls():
     """A smaller problem after a larger one: the shared scratch is cleared."""
-    big = synth.make_problem("cfg1", nx=90, ny=70, ndte=6)
+    big = synth.make_problem("grid400x300", nx=90, ny=70, ndte=6)
     small = synth.to_1d(synth.make_grid(41, 29, seed=11, ndte=6, curvilinear=True))
     for pr in (big, small, big):
         params = evp1d.set_evp_parameters(pr.ndte)
