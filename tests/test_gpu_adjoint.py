@@ -307,3 +307,25 @@ def test_adjoint_irregular_graph_matches_tape(oracle_mod, na, nhalo, seed):
         assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
     assert rel(g["uvel"], t["uvel0"]) < 1e-9
     assert rel(g["stress"], t["stress0"]) < 1e-9
+
+
+def test_adjoint_general_parameters_match_tape(oracle_mod):
+    """Every parameter branch at once (capping = 0, Ktens != 0, revised EVP,
+    a turning angle) with a nonzero seabed stress: gradients match the tape."""
+    import evp_tape
+    pr = small(seed=59, ndte=8)
+    rng = np.random.default_rng(9)
+    pr.f["Tbu"] = np.where(rng.uniform(size=pr.na) < 0.5, 0.0, rng.uniform(0.0, 2.0, pr.na))
+    p = evp1d.set_evp_parameters(pr.ndte)
+    p.capping, p.Ktens, p.revp = 0.0, 0.3, 1.0
+    p.cosw, p.sinw = float(np.cos(0.4)), float(np.sin(0.4))
+    uobs, vobs = synth.observations(pr.na, seed=12)
+    fs = evp1d.FieldSet.from_problem(pr)
+    with evp1d.EVP1D.from_problem(pr, params=p) as s:
+        s.run_checkpointed(pr.ndte, fs, 3)
+        g = s.adjoint(2 * (fs.uvel[: pr.na] - uobs), 2 * (fs.vvel[: pr.na] - vobs), stress=True)
+    t = evp_tape.gradient(pr, pr.ndte, p, uobs, vobs)
+    for k in FIELDS:
+        assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
+    assert rel(g["uvel"], t["uvel0"]) < 1e-9
+    assert rel(g["stress"], t["stress0"]) < 1e-9
