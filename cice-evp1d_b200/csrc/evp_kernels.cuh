@@ -76,11 +76,13 @@ void launch_fused(const FusedArgs &a, const Params &p, bool last,
 // Tbu, uinit, vinit).
 constexpr int kTmaStressFields = 19;
 constexpr int kTmaStepuFields = 13;
-// Per-call constants of a tile in one contiguous block (one bulk copy per
-// tile instead of twenty): kConstFields x kTileOwned doubles per tile, fields
-// [0..5] dxT dyT HTE HTN HTEm1 HTNm1, [6] strength, [7..19] the 13 stepu
-// inputs in the uf order, [20] meta | lcor << 32; unused slots hold 0.
-constexpr int kConstFields = 21;
+// Per-call constants of a tile in one contiguous block: kConstFields x
+// kTileOwned doubles per tile, fields [0..5] dxT dyT HTE HTN HTEm1 HTNm1,
+// [6] strength, [7] meta | lcor << 32 (the kConstStressFields that stress
+// reads), then [8..20] the 13 stepu inputs in the uf order; unused slots
+// hold 0.  Each of the two parts is one bulk copy.
+constexpr int kConstStressFields = 8;
+constexpr int kConstFields = kConstStressFields + kTmaStepuFields;
 constexpr int kConstTileSlots = kTileOwned;
 struct TmaArgs {
   int ntiles = 0;
@@ -104,8 +106,10 @@ struct TmaArgs {
   int *err = nullptr;  // nonzero after a bounded wait ran out
   int prefetch = 0;    // tiles prefetched into L2 ahead of the shared ring
   // optional timing trace of block 0 (debug): per tile 8 %globaltimer stamps
-  // [0] producer issued, [1] consumers have the stage, [2] stress done,
-  // [5] stepu done (3, 4, 6, 7 unused); kTraceTiles tiles at most
+  // [0] producers issued all copies, [1] consumer 0 has the stress part,
+  // [2] stress done (consumer barrier), [3] bulk warp has the tile record,
+  // [4] stress slot free, [5] consumer warp 0 done with stepu, [6] bulk
+  // copies issued, [7] gathers issued; kTraceTiles tiles at most
   long long *trace = nullptr;
 };
 constexpr int kTraceTiles = 256;
@@ -134,8 +138,9 @@ void launch_gather(const PermBatch &b, int na, const int32_t *slot_of_point,
 void launch_flags(int nslots, const int32_t *point_of_slot,
                   const int32_t *skipT, const int32_t *skipU, uint8_t *flags,
                   const uint32_t *lnb, uint32_t *meta, cudaStream_t st);
-// cblk[(t*kConstFields + f)*256 + l] = src[f][tile_off[t] + l] for l <
-// tile_cnt[t] (f < 20), meta | lcor << 32 for f = 20, and 0 for l >= tile_cnt.
+// cblk[(t*kConstFields + f)*256 + l] for l < tile_cnt[t] and slot
+// s = tile_off[t] + l: src[f][s] for f < 7, meta[s] | lcor[s] << 32 for f = 7,
+// src[f-1][s] for f >= 8; 0 for l >= tile_cnt[t].
 void launch_const_blocks(int ntiles, const int32_t *tile_off, const int32_t *tile_cnt,
                          const double *const src[kConstFields - 1], const uint32_t *meta,
                          const uint32_t *lcor, double *cblk, cudaStream_t st);

@@ -219,11 +219,11 @@ __global__ void k_const_blocks(int ntiles, const int32_t *tile_off, const int32_
     double v = 0.0;
     if (l < tile_cnt[t]) {
       const int s = tile_off[t] + l;
-      if (f < kConstFields - 1)
-        v = src.f[f][s];
-      else
+      if (f == kConstStressFields - 1)
         v = __longlong_as_double((long long)((unsigned long long)meta[s] |
                                              ((unsigned long long)lcor[s] << 32)));
+      else
+        v = src.f[f < kConstStressFields ? f : f - 1][s];
     }
     cblk[e] = v;
   }

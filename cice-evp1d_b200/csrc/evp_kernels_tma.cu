@@ -2,26 +2,33 @@
 // producer/consumer kernel (sm_100a).
 //
 // One CTA per SM walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
-// A producer warp stages each tile into a two-slot shared-memory ring:
-//   - the tile's owned points are contiguous slots, so each per-point field
-//     (7 stress inputs, 12 stresses, 13 stepu inputs, u, v and two packed
-//     index words) arrives with one cp.async.bulk (TMA) copy, completing on
-//     the stage's mbarrier with complete_tx;
-//   - the forward-halo points (recomputed stress) and the extra velocity
-//     points of the stencil are gathered with 4/8-byte cp.async, whose
-//     completion arrives on the same mbarrier (cp.async.mbarrier.arrive).
-// The producer's own inputs -- the tile's slot range and gather lists -- are
-// one 1.3 KB record per tile that a bulk copy brings kRecRing tiles ahead,
-// so the producer never waits on a global load.
+// A tile's inputs are staged in shared memory in two parts with different
+// lifetimes:
+//   - the stress part (geometry, strength, packed index words, the 12
+//     stresses, u and v of the owned points and of the stencil's extra
+//     points, and the recomputed forward halo) is dead once stress is done;
+//     it has a three-slot ring, so two later tiles load while one computes;
+//   - the stepu part (the 13 stepu inputs) has one slot, loaded while the
+//     consumers compute the tile's stress.
+// The owned points of a tile are contiguous slots and its per-call constants
+// one contiguous block, so the owned data arrive by cp.async.bulk (TMA)
+// copies completing on the slot's mbarrier (complete_tx); the halo and the
+// extra velocities are gathered with 4/8-byte cp.async, whose completion
+// arrives on the same mbarrier (cp.async.mbarrier.arrive).
+// Producer warps: the bulk warp (the bulk copies of both parts) and
+// kGatherWarps gather warps issuing the cp.async gathers side by side with it.  The producers' own inputs -- the
+// tile's slot range and gather lists -- are one 1.3 KB record per tile that a
+// bulk copy brings kRecRing tiles ahead, so no producer waits on a global
+// load.
 // Ten consumer warps (one thread per compute-set point: 256 owned + 64 halo)
 // compute stress from shared memory into the shared str table, then stepu for
 // the owned points, writing the new stresses and velocities to the other
-// ping-pong buffer.  While they compute tile k the producer loads tile k+1.
+// ping-pong buffer.
 //
 // Every mbarrier wait is bounded by %globaltimer (kWaitNs): on expiry the
 // kernel records an error code, every thread of the consumer group leaves the
-// tile loop together, and the producer waits (bounded) for the copies it has
-// issued before it exits, so nothing is left in flight.
+// tile loop together, and each producer warp waits (bounded) for the copies it
+// has issued before it exits, so nothing is left in flight.
 #include <cstdint>
 
 #include "evp_kernels.cuh"
@@ -31,40 +38,53 @@ namespace evp {
 
 namespace {
 
-constexpr int kStages = 2;
+constexpr int kSSlots = 2;                          // stress-part ring
 constexpr int kRecRing = 4;                         // producer records in flight
 constexpr int kConsumers = kTileOwned + kTileHalo;  // 320 = 10 warps
-constexpr int kThreads = kConsumers + 32;           // + 1 producer warp
+constexpr int kGatherWarps = 2;                     // producer warps issuing cp.async gathers
+constexpr int kStageWarps = 1 + kGatherWarps;       // bulk warp + gather warps
+constexpr int kThreads = kConsumers + 32 * kStageWarps;
 constexpr int kUV = kTileOwned + kTileUvx;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s
 
-struct Stage {
-  double cf[kConstFields][kTileOwned];  // the tile's constant block (one bulk copy)
-  double s12[12][kTileOwned];           // the 12 stresses
+// Stress part of a tile.
+struct SSlot {
+  double cs[kConstStressFields][kTileOwned];  // constant block fields 0..7 (one bulk copy)
+  double s12[12][kTileOwned];                 // the 12 stresses
   double u[kUV];
   double v[kUV];
   double hf[kTmaStressFields][kTileHalo];  // halo: 6 geometry, strength, 12 stresses
   uint32_t hmeta[kTileHalo];
   uint32_t hlcc[kTileHalo];
   uint32_t hlcor[kTileHalo];
-  int hdr[4];  // tile offset, owned count, halo count (written by the producer)
+  int hdr[4];  // tile offset, owned count, halo count (written by the bulk warp)
+};
+
+// Stepu part of a tile: constant block fields 8..20 (one bulk copy).
+struct USlot {
+  double cu[kTmaStepuFields][kTileOwned];
 };
 
 static_assert(kConstTileSlots == kTileOwned, "constant blocks hold one tile");
-static_assert(kConstFields == 7 + kTmaStepuFields + 1, "constant block layout");
+static_assert(kConstFields == kConstStressFields + kTmaStepuFields, "constant block layout");
 
 struct Smem {
-  Stage st[kStages];
-  double str[8][kZeroSlot + 2];
+  SSlot ss[kSSlots];
+  USlot us;
+  double str[2][8][kZeroSlot + 2];  // double-buffered str table
   int32_t rec[kRecRing][kRecInts];
-  unsigned long long full[kStages];
-  unsigned long long empty[kStages];
+  unsigned long long sfull[kSSlots];
+  unsigned long long sempty[kSSlots];
+  unsigned long long ufull, uempty;
   unsigned long long rec_full[kRecRing];
   int abort_flag;
+  int prod_ok;  // the bulk warp's waits succeeded for the current tile
 };
 
-static_assert(sizeof(Stage) % 16 == 0, "stage must keep 16-byte alignment");
+static_assert(sizeof(SSlot) % 16 == 0 && sizeof(USlot) % 16 == 0,
+              "slots must keep 16-byte alignment");
 static_assert((kRecInts * 4) % 16 == 0, "records are bulk-copied");
+static_assert(sizeof(Smem) <= 227 * 1024, "shared memory per block");
 
 // ---------------- PTX helpers -------------------------------------------------
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -160,12 +180,35 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-__device__ __forceinline__ void consumer_sync() {
-  asm volatile("bar.sync 1, %0;" ::"r"(kConsumers) : "memory");
+// Barrier of the consumer warps that also ORs a predicate over them.
+__device__ __forceinline__ bool consumer_sync_or(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(kConsumers)
+      : "memory");
+  return r != 0;
+}
+
+// The bulk warp and the gather warps.
+__device__ __forceinline__ void stage_sync() {
+  asm volatile("bar.sync 2, %0;" ::"r"(32 * kStageWarps) : "memory");
 }
 
 __device__ __forceinline__ void trace_stamp(const TmaArgs &a, int it, int slot) {
   if (a.trace && blockIdx.x == 0 && it < kTraceTiles) a.trace[it * 8 + slot] = (long long)global_ns();
+}
+
+// The stepu part of tile t (constant block fields 8..20) into the stepu slot.
+__device__ __forceinline__ void issue_stepu(const TmaArgs &a, Smem &S, int t) {
+  constexpr uint32_t kBytes = kTmaStepuFields * kTileOwned * 8u;
+  mbar_arrive_expect_tx(&S.ufull, kBytes);
+  bulk_g2s(S.us.cu, a.cblk + ((size_t)t * kConstFields + kConstStressFields) * kTileOwned, kBytes,
+           &S.ufull);
 }
 
 // ---------------- the kernel ---------------------------------------------------
@@ -183,23 +226,45 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     return;
   }
   if (tid == 0) {
-    for (int s = 0; s < kStages; s++) {
-      mbar_init(&S.full[s], 1 + 32);  // expect_tx arrival + 32 cp.async lanes
-      mbar_init(&S.empty[s], 1);      // one consumer arrival per use
+    for (int s = 0; s < kSSlots; s++) {
+      mbar_init(&S.sfull[s], 1 + 32 * kGatherWarps);  // expect_tx arrival + cp.async lanes
+      mbar_init(&S.sempty[s], 1);                     // one consumer arrival per use
     }
+    mbar_init(&S.ufull, 1);
+    mbar_init(&S.uempty, kConsumers / 32);  // one arrival per consumer warp
     for (int r = 0; r < kRecRing; r++) mbar_init(&S.rec_full[r], 1);
     S.abort_flag = 0;
     mbar_fence_init();
   }
-  if (tid < 8) S.str[tid][kZeroSlot] = 0.0;
+  if (tid < 16) S.str[tid >> 3][tid & 7][kZeroSlot] = 0.0;
   __syncthreads();
 
+  const int T0 = blockIdx.x, dT = gridDim.x;
+  constexpr uint32_t kCsBytes = kConstStressFields * kTileOwned * 8u;
+  constexpr size_t kBlk = (size_t)kConstFields * kTileOwned;  // doubles per constant block
+
   if (tid >= kConsumers) {
-    // ======================= producer warp ==============================
-    const int lane = tid - kConsumers;
-    const int T0 = blockIdx.x, dT = gridDim.x;
+    // ======================= producers ===================================
+    // The bulk warp (pw 0) waits for the tile record and the free slot,
+    // writes the slot header, arms the slot's full barrier and issues the
+    // bulk copies (TMA unit); the gather warps meanwhile issue the 8-byte
+    // cp.async gathers of the forward halo and the extra velocities
+    // (load/store path).  Two named-barrier handshakes per tile order the
+    // warps: after the first the slot is armed and the record readable, after
+    // the second every warp is done with the record, which the bulk warp then
+    // refills.  The bulk warp's waits are bounded and it reaches the first
+    // handshake on every path, so the handshakes cannot hang; a failed wait
+    // is passed on through prod_ok.
+    // The bulk warp also issues the stepu part: tile i's stress part goes
+    // out two tiles ahead of its use, tile j's stepu part as soon as the
+    // stepu slot is free (end of stepu(j-1)).  The TMA unit serves the
+    // copies in issue order, so in round i the stepu part of tile i-2 is
+    // issued before the stress part of tile i (whose slot was freed earlier,
+    // at the end of stress(i-3)), which keeps the urgent copy at the front.
+    const int pw = (tid - kConsumers) >> 5;
+    const int lane = tid & 31;
     constexpr uint32_t kRecBytes = kRecInts * 4u;
-    if (lane == 0) {
+    if (pw == 0 && lane == 0) {
       for (int r = 0; r < kRecRing; r++) {
         const int t = T0 + r * dT;
         if (t >= a.ntiles) break;
@@ -208,94 +273,139 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       }
     }
     int issued = 0;
+    int nu = 0;  // stepu parts issued (counted by the bulk warp's lane 0)
     bool ok = true;
     for (int t = T0; t < a.ntiles; t += dT) {
       const int r = issued % kRecRing;
-      int w = 1;
-      if (lane == 0) w = mbar_wait(&S.rec_full[r], (uint32_t)(issued / kRecRing) & 1, a.err, 6);
-      const int s = issued % kStages;
-      const uint32_t use = (uint32_t)(issued / kStages);
-      if (w && issued >= kStages && lane == 0)
-        w = mbar_wait(&S.empty[s], (use - 1) & 1, a.err, 2) ? 1 : 0;
-      w = __shfl_sync(0xffffffffu, w, 0);
-      if (!w) {
+      const int s = issued % kSSlots;
+      const uint32_t use = (uint32_t)(issued / kSSlots);
+      SSlot &st = S.ss[s];
+      const int32_t *rec = S.rec[r];
+      if (pw == 0) {
+        int w = 1;
+        if (lane == 0) {
+          w = mbar_wait(&S.rec_full[r], (uint32_t)(issued / kRecRing) & 1, a.err, 6) ? 1 : 0;
+          trace_stamp(a, issued, 3);
+          if (w && issued >= kSSlots) {
+            // stepu part nu == issued - 2; its slot frees after stepu(nu - 1)
+            w = mbar_wait(&S.uempty, (uint32_t)(nu - 1) & 1, a.err, 9) ? 1 : 0;
+            if (w) issue_stepu(a, S, T0 + (nu++) * dT);
+            if (w) w = mbar_wait(&S.sempty[s], (use - 1) & 1, a.err, 2) ? 1 : 0;
+          }
+          trace_stamp(a, issued, 4);
+        }
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w) {
+          const int nh = rec[3];
+          for (int h = lane; h < nh; h += 32) {
+            st.hlcor[h] = (uint32_t)rec[kRecHLcor + h];
+            st.hlcc[h] = (uint32_t)rec[kRecHLcc + h];
+          }
+          if (lane == 0) {
+            st.hdr[0] = rec[0];
+            st.hdr[1] = rec[1];
+            st.hdr[2] = nh;
+          }
+          __syncwarp();
+          // release: the header and halo indices are visible to consumers
+          // once the phase completes
+          if (lane == 0) {
+            const uint32_t b8 = (uint32_t)((rec[1] + 3) & ~3) * 8u;
+            mbar_arrive_expect_tx(&S.sfull[s], kCsBytes + 14 * b8);
+          }
+        }
+        if (lane == 0) S.prod_ok = w;
+      }
+      stage_sync();  // handshake 1
+      if (!S.prod_ok) {
         ok = false;
         break;
       }
-      const int32_t *rec = S.rec[r];
       const int off = rec[0], cnt = rec[1], nx = rec[2], nh = rec[3];
-      Stage &st = S.st[s];
-      for (int h = lane; h < nh; h += 32) {
-        st.hlcor[h] = (uint32_t)rec[kRecHLcor + h];
-        st.hlcc[h] = (uint32_t)rec[kRecHLcc + h];
+      if (pw == 0) {
+        const uint32_t b8 = (uint32_t)((cnt + 3) & ~3) * 8u;
+        if (lane == 0)
+          bulk_g2s(st.cs, a.cblk + (size_t)t * kBlk, kCsBytes, &S.sfull[s]);
+        else if (lane <= 12)
+          bulk_g2s(st.s12[lane - 1], a.sf[6 + lane] + off, b8, &S.sfull[s]);
+        else if (lane == 13)
+          bulk_g2s(st.u, a.u_in + off, b8, &S.sfull[s]);
+        else if (lane == 14)
+          bulk_g2s(st.v, a.v_in + off, b8, &S.sfull[s]);
+        if (lane == 0) {
+          if (issued == 0) issue_stepu(a, S, T0 + (nu++) * dT);
+          trace_stamp(a, issued, 6);
+        }
+      } else {
+        // gather warp gw takes the velocity extras u (first) / v (last) and
+        // every kGatherWarps-th halo field; the last one also the halo meta
+        const int gw = pw - 1;
+        if (gw == 0)
+          for (int x = lane; x < nx; x += 32)
+            cp_async8(&st.u[kTileOwned + x], a.u_in + rec[kRecUvx + x]);
+        if (gw == kGatherWarps - 1)
+          for (int x = lane; x < nx; x += 32)
+            cp_async8(&st.v[kTileOwned + x], a.v_in + rec[kRecUvx + x]);
+        for (int h = lane; h < nh; h += 32) {
+          const int g = rec[kRecHalo + h];
+          for (int f = gw; f < kTmaStressFields; f += kGatherWarps) cp_async8(&st.hf[f][h], a.sf[f] + g);
+          if (gw == kGatherWarps - 1) cp_async4(&st.hmeta[h], a.meta + g);
+        }
+        cp_async_arrive(&S.sfull[s]);
+        if (gw == 0 && lane == 0) trace_stamp(a, issued, 7);
       }
-      if (lane == 0) {
-        st.hdr[0] = off;
-        st.hdr[1] = cnt;
-        st.hdr[2] = nh;
-      }
-      __syncwarp();
-      const uint32_t n4 = (uint32_t)((cnt + 3) & ~3);
-      const uint32_t b8 = n4 * 8u;
-      constexpr uint32_t kConstBytes = kConstFields * kTileOwned * 8u;
-      // release: the header and halo indices are visible to consumers once
-      // the phase completes
-      if (lane == 0) mbar_arrive_expect_tx(&S.full[s], kConstBytes + 14 * b8);
-      __syncwarp();
-      if (lane == 0)
-        bulk_g2s(st.cf, a.cblk + (size_t)t * kConstFields * kTileOwned, kConstBytes, &S.full[s]);
-      else if (lane <= 12)
-        bulk_g2s(st.s12[lane - 1], a.sf[6 + lane] + off, b8, &S.full[s]);
-      else if (lane == 13)
-        bulk_g2s(st.u, a.u_in + off, b8, &S.full[s]);
-      else if (lane == 14)
-        bulk_g2s(st.v, a.v_in + off, b8, &S.full[s]);
-      for (int x = lane; x < nx; x += 32) {
-        const int g = rec[kRecUvx + x];
-        cp_async8(&st.u[kTileOwned + x], a.u_in + g);
-        cp_async8(&st.v[kTileOwned + x], a.v_in + g);
-      }
-      for (int h = lane; h < nh; h += 32) {
-        const int g = rec[kRecHalo + h];
-        for (int f = 0; f < kTmaStressFields; f++) cp_async8(&st.hf[f][h], a.sf[f] + g);
-        cp_async4(&st.hmeta[h], a.meta + g);
-      }
-      cp_async_arrive(&S.full[s]);
-      if (lane == 0) trace_stamp(a, issued, 0);
-      // record slot r has been read: refill it kRecRing tiles ahead
+      // the record's generic reads come before its async-proxy refill
       fence_proxy_async();
-      __syncwarp();
-      const int tr = t + kRecRing * dT;
-      if (lane == 0 && tr < a.ntiles) {
-        mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
-        bulk_g2s(S.rec[r], a.tile_rec + (size_t)tr * kRecInts, kRecBytes, &S.rec_full[r]);
-      }
-      if (a.prefetch > 0) {
-        const int tp = t + a.prefetch * dT;
-        if (tp < a.ntiles && lane < 2) {
-          // the owned slot range of every staged field of a later tile
-          const int po = a.tile_meta[8 * tp], pc = a.tile_meta[8 * tp + 1];
-          const uint32_t pn = (uint32_t)((pc + 3) & ~3);
-          for (int f = lane; f < kTmaStressFields; f += 2) bulk_prefetch_l2(a.sf[f] + po, pn * 8u);
-          for (int f = lane; f < kTmaStepuFields; f += 2) bulk_prefetch_l2(a.uf[f] + po, pn * 8u);
+      stage_sync();  // handshake 2
+      if (pw == 0) {
+        if (lane == 0) trace_stamp(a, issued, 0);
+        const int tr = t + kRecRing * dT;
+        if (lane == 0 && tr < a.ntiles) {
+          mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
+          bulk_g2s(S.rec[r], a.tile_rec + (size_t)tr * kRecInts, kRecBytes, &S.rec_full[r]);
+        }
+        if (a.prefetch > 0) {
+          const int tp = t + a.prefetch * dT;
+          if (tp < a.ntiles && lane < 15) {
+            // what the stage load of a later tile copies: its constant block,
+            // the owned ranges of the 12 stresses, u and v
+            const int po = a.tile_meta[8 * tp], pc = a.tile_meta[8 * tp + 1];
+            const uint32_t pb = (uint32_t)((pc + 3) & ~3) * 8u;
+            if (lane == 0)
+              bulk_prefetch_l2(a.cblk + (size_t)tp * kBlk, (uint32_t)(kBlk * 8u));
+            else if (lane <= 12)
+              bulk_prefetch_l2(a.sf[6 + lane] + po, pb);
+            else
+              bulk_prefetch_l2((lane == 13 ? a.u_in : a.v_in) + po, pb);
+          }
         }
       }
       issued++;
     }
-    if (!ok) {
-      // Consumers stopped early: wait (bounded) until every issued stage has
-      // landed so that no copy targets shared memory after the CTA exits.
-      for (int k = issued - kStages; k < issued; k++) {
-        if (k < 0) continue;
-        if (lane == 0) mbar_wait(&S.full[k % kStages], (uint32_t)(k / kStages) & 1, a.err, 3);
+    if (pw == 0) {
+      if (ok && lane == 0) {
+        // the stepu parts of the last tiles
+        for (; nu < issued; nu++) {
+          if (!mbar_wait(&S.uempty, (uint32_t)(nu - 1) & 1, a.err, 9)) break;
+          issue_stepu(a, S, T0 + nu * dT);
+        }
       }
-    }
-    // records issued ahead and never consumed must land before exit too
-    if (lane == 0) {
-      for (int k = issued; k < issued + kRecRing; k++) {
-        const int t = T0 + k * dT;
-        if (t >= a.ntiles) break;
-        mbar_wait(&S.rec_full[k % kRecRing], (uint32_t)(k / kRecRing) & 1, a.err, 7);
+      if (lane == 0 && nu > 0) mbar_wait(&S.ufull, (uint32_t)(nu - 1) & 1, a.err, 10);
+      if (!ok) {
+        // Consumers stopped early: wait (bounded) until every issued slot has
+        // landed so that no copy targets shared memory after the CTA exits.
+        for (int k = issued - kSSlots; k < issued; k++) {
+          if (k < 0) continue;
+          if (lane == 0) mbar_wait(&S.sfull[k % kSSlots], (uint32_t)(k / kSSlots) & 1, a.err, 3);
+        }
+      }
+      // records issued ahead and never consumed must land before exit too
+      if (lane == 0) {
+        for (int k = issued; k < issued + kRecRing; k++) {
+          const int t = T0 + k * dT;
+          if (t >= a.ntiles) break;
+          mbar_wait(&S.rec_full[k % kRecRing], (uint32_t)(k / kRecRing) & 1, a.err, 7);
+        }
       }
     }
     __syncwarp();
@@ -303,119 +413,143 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   }
 
   // ========================= consumers ===================================
+  // Per tile one block barrier: after stress, when the tile's str table is
+  // complete.  Stepu then runs warp by warp and each warp goes straight on to
+  // the next tile's stress, so one warp's stepu overlaps the others' stress;
+  // str is double-buffered (stress of tile k+1 writes the other table, and
+  // every warp has finished stepu(k-1) before any passes the barrier of tile
+  // k).  The stepu slot is released by one arrival per warp.  A wait that ran
+  // out anywhere is OR-reduced at the barrier, so all consumers leave the
+  // loop together.
   const int c = tid;  // compute-set index: owned c < 256, halo 256 + h
+  const int lane = tid & 31;
+  bool fail = false;
   int it = 0;
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, it++) {
-    const int s = it % kStages;
-    const uint32_t use = (uint32_t)(it / kStages);
-    if (!mbar_wait(&S.full[s], use & 1, a.err, 1)) S.abort_flag = 1;
-    consumer_sync();
-    if (S.abort_flag) break;
+  for (int t = T0; t < a.ntiles; t += dT, it++) {
+    const int s = it % kSSlots;
+    const int b = it & 1;
+    const bool have = mbar_wait(&S.sfull[s], (uint32_t)(it / kSSlots) & 1, a.err, 1);
+    fail |= !have;
     if (tid == 0) trace_stamp(a, it, 1);
-    const Stage &st = S.st[s];
-    const int off = st.hdr[0], cnt = st.hdr[1], nh = st.hdr[2];
+    const SSlot &st = S.ss[s];
 
     // ---------------- phase 1: stress ------------------------------------
+    // The owned thread keeps what stepu needs from the stress part (its
+    // index word and velocity) so that the slot can be released after stress.
     const bool own = c < kTileOwned;
     const int h = c - kTileOwned;
-    if (own ? c < cnt : h < nh) {
-      uint32_t m, lc;
-      if (own) {
-        const unsigned long long ml = (unsigned long long)__double_as_longlong(st.cf[20][c]);
-        m = (uint32_t)ml;
-        lc = (uint32_t)(ml >> 32);
-      } else {
-        m = st.hmeta[h];
-        lc = st.hlcor[h];
-      }
-      double out[8];
-      if ((m >> 30) & kSkipT) {
-#pragma unroll
-        for (int k = 0; k < 8; k++) out[k] = 0.0;
-      } else {
-        // geometry and strength (fields 0..6), then the 12 stresses
-        const double *F = own ? &st.cf[0][c] : &st.hf[0][h];
-        const double *F12 = own ? &st.s12[0][c] : &st.hf[7][h];
-        const int fs = own ? kTileOwned : kTileHalo;
-        const int cc = own ? c : (int)st.hlcc[h];
-        const int iee = lc & kLnbMask, ine = (lc >> kLnbBits) & kLnbMask;
-        const int ise = (lc >> (2 * kLnbBits)) & kLnbMask;
-        Corners cr;
-        cr.ucc = st.u[cc];
-        cr.vcc = st.v[cc];
-        cr.uee = st.u[iee];
-        cr.vee = st.v[iee];
-        cr.une = st.u[ine];
-        cr.vne = st.v[ine];
-        cr.use = st.u[ise];
-        cr.vse = st.v[ise];
-        const Geom gm = make_geom(F[0 * fs], F[1 * fs], F[2 * fs], F[3 * fs], F[4 * fs],
-                                  F[5 * fs], p.deltaminEVP);
-        const Strain sr = strain_rates(cr, gm, p.e_factor);
-        double s12[12];
-#pragma unroll
-        for (int k = 0; k < 12; k++) s12[k] = F12[k * fs];
-        stress_update(s12, out, sr, F[6 * fs], gm, p);
+    uint32_t m = 0;
+    double uold = 0.0, vold = 0.0;
+    int off = 0, cnt = 0;
+    if (have) {
+      off = st.hdr[0];
+      cnt = st.hdr[1];
+      const int nh = st.hdr[2];
+      if (own ? c < cnt : h < nh) {
+        uint32_t lc;
         if (own) {
-#pragma unroll
-          for (int k = 0; k < 12; k++) a.s_out[k][off + c] = s12[k];
+          const unsigned long long ml = (unsigned long long)__double_as_longlong(st.cs[7][c]);
+          m = (uint32_t)ml;
+          lc = (uint32_t)(ml >> 32);
+          uold = st.u[c];
+          vold = st.v[c];
+        } else {
+          m = st.hmeta[h];
+          lc = st.hlcor[h];
         }
-      }
+        double out[8];
+        if ((m >> 30) & kSkipT) {
 #pragma unroll
-      for (int k = 0; k < 8; k++) S.str[k][c] = out[k];
-      if (kLast && own) {
+          for (int k = 0; k < 8; k++) out[k] = 0.0;
+        } else {
+          // geometry and strength (fields 0..6), then the 12 stresses
+          const double *F = own ? &st.cs[0][c] : &st.hf[0][h];
+          const double *F12 = own ? &st.s12[0][c] : &st.hf[7][h];
+          const int fs = own ? kTileOwned : kTileHalo;
+          const int cc = own ? c : (int)st.hlcc[h];
+          const int iee = lc & kLnbMask, ine = (lc >> kLnbBits) & kLnbMask;
+          const int ise = (lc >> (2 * kLnbBits)) & kLnbMask;
+          Corners cr;
+          cr.ucc = st.u[cc];
+          cr.vcc = st.v[cc];
+          cr.uee = st.u[iee];
+          cr.vee = st.v[iee];
+          cr.une = st.u[ine];
+          cr.vne = st.v[ine];
+          cr.use = st.u[ise];
+          cr.vse = st.v[ise];
+          const Geom gm = make_geom(F[0 * fs], F[1 * fs], F[2 * fs], F[3 * fs], F[4 * fs],
+                                    F[5 * fs], p.deltaminEVP);
+          const Strain sr = strain_rates(cr, gm, p.e_factor);
+          double s12[12];
 #pragma unroll
-        for (int k = 0; k < 8; k++) a.str_out[k][off + c] = out[k];
-      }
-    }
-    consumer_sync();
-    if (tid == 0) trace_stamp(a, it, 2);
-
-    // ---------------- phase 2: stepu on owned points ------------------------
-    if (c < cnt) {
-      const uint32_t m = (uint32_t)__double_as_longlong(st.cf[20][c]);
-      if (!((m >> 30) & kSkipU)) {
-        const int lnw = m & kLnbMask, lsw = (m >> kLnbBits) & kLnbMask;
-        const int lsse = (m >> (2 * kLnbBits)) & kLnbMask;
-        StepuIn in;
-        in.uold = st.u[c];
-        in.vold = st.v[c];
-        in.kvrel = st.cf[7][c];
-        in.uocn = st.cf[8][c];
-        in.vocn = st.cf[9][c];
-        in.waterx = st.cf[10][c];
-        in.watery = st.cf[11][c];
-        in.forcex = st.cf[12][c];
-        in.forcey = st.cf[13][c];
-        in.umassdti = st.cf[14][c];
-        in.fm = st.cf[15][c];
-        in.uarear = st.cf[16][c];
-        in.Tbu = st.cf[17][c];
-        in.uinit = st.cf[18][c];
-        in.vinit = st.cf[19][c];
-        in.s1 = S.str[0][c];
-        in.s2nw = S.str[1][lnw];
-        in.s3sse = S.str[2][lsse];
-        in.s4sw = S.str[3][lsw];
-        in.s5 = S.str[4][c];
-        in.s6sse = S.str[5][lsse];
-        in.s7nw = S.str[6][lnw];
-        in.s8sw = S.str[7][lsw];
-        const StepuOut o = stepu_point(in, p);
-        a.u_out[off + c] = o.u;
-        a.v_out[off + c] = o.v;
-        if (kLast) {
-          a.strintx[off + c] = o.strintx;
-          a.strinty[off + c] = o.strinty;
-          a.Cb[off + c] = o.Cb;
+          for (int k = 0; k < 12; k++) s12[k] = F12[k * fs];
+          stress_update(s12, out, sr, F[6 * fs], gm, p);
+          if (own) {
+#pragma unroll
+            for (int k = 0; k < 12; k++) a.s_out[k][off + c] = s12[k];
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) S.str[b][k][c] = out[k];
+        if (kLast && own) {
+#pragma unroll
+          for (int k = 0; k < 8; k++) a.str_out[k][off + c] = out[k];
         }
       }
     }
-    consumer_sync();  // stage s and the str table are free again
+    // str of this tile complete; the stress part of slot s is free again
+    const bool stop = consumer_sync_or(fail);
     if (tid == 0) {
-      trace_stamp(a, it, 5);
-      mbar_arrive(&S.empty[s]);
+      trace_stamp(a, it, 2);
+      mbar_arrive(&S.sempty[s]);
     }
+    if (stop) break;
+
+    // ---------------- phase 2: stepu on owned points, warp by warp ----------
+    const bool hu = mbar_wait(&S.ufull, (uint32_t)it & 1, a.err, 11);
+    fail |= !hu;
+    if (hu && c < cnt && !((m >> 30) & kSkipU)) {
+      const USlot &us = S.us;
+      const double(&str)[8][kZeroSlot + 2] = S.str[b];
+      const int lnw = m & kLnbMask, lsw = (m >> kLnbBits) & kLnbMask;
+      const int lsse = (m >> (2 * kLnbBits)) & kLnbMask;
+      StepuIn in;
+      in.uold = uold;
+      in.vold = vold;
+      in.kvrel = us.cu[0][c];
+      in.uocn = us.cu[1][c];
+      in.vocn = us.cu[2][c];
+      in.waterx = us.cu[3][c];
+      in.watery = us.cu[4][c];
+      in.forcex = us.cu[5][c];
+      in.forcey = us.cu[6][c];
+      in.umassdti = us.cu[7][c];
+      in.fm = us.cu[8][c];
+      in.uarear = us.cu[9][c];
+      in.Tbu = us.cu[10][c];
+      in.uinit = us.cu[11][c];
+      in.vinit = us.cu[12][c];
+      in.s1 = str[0][c];
+      in.s2nw = str[1][lnw];
+      in.s3sse = str[2][lsse];
+      in.s4sw = str[3][lsw];
+      in.s5 = str[4][c];
+      in.s6sse = str[5][lsse];
+      in.s7nw = str[6][lnw];
+      in.s8sw = str[7][lsw];
+      const StepuOut o = stepu_point(in, p);
+      a.u_out[off + c] = o.u;
+      a.v_out[off + c] = o.v;
+      if (kLast) {
+        a.strintx[off + c] = o.strintx;
+        a.strinty[off + c] = o.strinty;
+        a.Cb[off + c] = o.Cb;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&S.uempty);  // this warp is done with the stepu slot
+    if (tid == 0) trace_stamp(a, it, 5);
   }
 }
 

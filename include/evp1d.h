@@ -164,9 +164,11 @@ int evp1d_synchronize(evp1d_t *handle);
 
 /* Debug: timing trace of the TMA kernel's block 0 in the last launch
  * (recorded only when EVP1D_TRACE is set at evp1d_init).  Up to 256 tiles x 8
- * %globaltimer stamps (ns): [0] producer issued the tile's copies, [1] the
- * consumers have the stage, [2] stress done, [5] stepu done; 3, 4, 6, 7
- * unused (0). */
+ * %globaltimer stamps (ns): [0] the producer warps issued all of the tile's
+ * copies, [1] consumer 0 has the tile's stress inputs, [2] stress done (all
+ * consumers), [3] the bulk-copy warp has the tile record, [4] the tile's
+ * stress slot is free, [5] consumer warp 0 finished stepu, [6] bulk copies
+ * issued, [7] halo gathers issued. */
 int evp1d_debug_trace(evp1d_t *handle, long long *out, int n);
 
 /* Name of the subcycle kernel the handle runs: "fused-tile-tma" (default,
