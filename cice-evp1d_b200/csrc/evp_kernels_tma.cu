@@ -212,7 +212,8 @@ __device__ __forceinline__ void issue_stepu(const TmaArgs &a, Smem &S, int t) {
 }
 
 // ---------------- the kernel ---------------------------------------------------
-template <bool kLast>
+// kStd: parameters with std_params(p) (stress_update_std).
+template <bool kLast, bool kStd>
 __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   // Indexed straight off the __shared__ symbol (no integer round trip), so
   // every access compiles to a shared-memory load or store, not a generic one.
@@ -484,7 +485,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
           double s12[12];
 #pragma unroll
           for (int k = 0; k < 12; k++) s12[k] = F12[k * fs];
-          stress_update(s12, out, sr, F[6 * fs], gm, p);
+          if (kStd)
+            stress_update_std(s12, out, sr, F[6 * fs], gm, p);
+          else
+            stress_update(s12, out, sr, F[6 * fs], gm, p);
           if (own) {
 #pragma unroll
             for (int k = 0; k < 12; k++) a.s_out[k][off + c] = s12[k];
@@ -559,9 +563,11 @@ size_t smem_bytes() { return sizeof(Smem); }
 
 int tma_prepare(int device) {
   const int bytes = (int)smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(k_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  void (*const ks[4])(TmaArgs, Params) = {k_tma<false, false>, k_tma<true, false>,
+                                          k_tma<false, true>, k_tma<true, true>};
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 4 && e == cudaSuccess; i++)
+    e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   (void)device;
   return e == cudaSuccess ? 0 : (int)e;
 }
@@ -569,10 +575,15 @@ int tma_prepare(int device) {
 void launch_tma(const TmaArgs &a, const Params &p, bool last, int nctas, cudaStream_t st) {
   if (a.ntiles <= 0) return;
   const int grid = a.ntiles < nctas ? a.ntiles : nctas;
-  if (last)
-    k_tma<true><<<grid, kThreads, smem_bytes(), st>>>(a, p);
+  const bool std = std_params(p);
+  if (last && std)
+    k_tma<true, true><<<grid, kThreads, smem_bytes(), st>>>(a, p);
+  else if (last)
+    k_tma<true, false><<<grid, kThreads, smem_bytes(), st>>>(a, p);
+  else if (std)
+    k_tma<false, true><<<grid, kThreads, smem_bytes(), st>>>(a, p);
   else
-    k_tma<false><<<grid, kThreads, smem_bytes(), st>>>(a, p);
+    k_tma<false, false><<<grid, kThreads, smem_bytes(), st>>>(a, p);
 }
 
 }  // namespace evp

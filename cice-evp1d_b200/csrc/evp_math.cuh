@@ -196,6 +196,45 @@ __host__ __device__ __forceinline__ void stress_update(
   str_combine(s, out, g);
 }
 
+// True when stress_update_std may replace stress_update: capping == 1,
+// Ktens == 0, revp == 0 and a finite arlx1i.
+__host__ __device__ __forceinline__ bool std_params(const Params &p) {
+  return p.capping == kC1 && p.Ktens == 0.0 && p.revp == 0.0 && p.arlx1i - p.arlx1i == 0.0;
+}
+
+// stress_update for parameters with std_params(p), as straight-line code: the
+// four corners' divisions carry no per-corner branch, so they can overlap.
+// Exactly the bits of stress_update:
+//  - the capping shortcut of visc_replpress holds for all four corners when
+//    DminTarea > 0, |strength| < 1e300*DminTarea and no Delta is NaN; those
+//    conditions are tested once and, if any fails (never in normal runs),
+//    the general stress_update runs instead on the unchanged stresses;
+//  - revp == 0 with a finite arlx1i makes (1 - arlx1i*revp) exactly 1, and
+//    x*1 is x for every x, so that product is dropped.
+__host__ __device__ __forceinline__ void stress_update_std(
+    double (&s)[12], double (&out)[8], const Strain &sr, double strength,
+    const Geom &g, const Params &p) {
+  const double DminArea = g.DminTarea;
+  const bool ok = DminArea > 0.0 && fabs(strength) < 1e300 * DminArea &&
+                  sr.Delta[0] == sr.Delta[0] && sr.Delta[1] == sr.Delta[1] &&
+                  sr.Delta[2] == sr.Delta[2] && sr.Delta[3] == sr.Delta[3];
+  if (!ok) {
+    stress_update(s, out, sr, strength, g, p);
+    return;
+  }
+  const double arlx1i = p.arlx1i, denom1 = p.denom1;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const double z = strength / fmax_ref(sr.Delta[k], DminArea);
+    const double r = z * sr.Delta[k];
+    const double e = p.epp2i * z;
+    s[k] = (s[k] + arlx1i * (z * sr.div[k] - r)) * denom1;
+    s[4 + k] = (s[4 + k] + arlx1i * e * sr.ten[k]) * denom1;
+    s[8 + k] = (s[8 + k] + arlx1i * kP5 * e * sr.shr[k]) * denom1;
+  }
+  str_combine(s, out, g);
+}
+
 __host__ __device__ __forceinline__ void str_combine(const double (&s)[12],
                                                      double (&out)[8],
                                                      const Geom &g) {
