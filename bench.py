@@ -715,7 +715,14 @@ def main():
                          "traffic": alg_bytes.measured_traffic(ROOT, path, args.config),
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_point_subcycle": ab,
-                         "kernel": path},
+                         "kernel": path,
+                         # the same rate over the reference's unfused data
+                         # contract (str1..8 through HBM, 576 B): what the
+                         # reference's two kernels would have to move
+                         "reference_contract": {
+                             "bytes_per_point_subcycle": alg_bytes.per_point_subcycle("two-kernel"),
+                             "equivalent_gbs": alg_bytes.per_point_subcycle("two-kernel") * pr.n_active / sub_s / 1e9,
+                             "equivalent_frac": alg_bytes.per_point_subcycle("two-kernel") * pr.n_active / sub_s / 1e9 / peak}},
             "e2e": {"value": e2e_value, "unit": UNIT, "host_memory": "page-locked",
                     "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
