@@ -286,6 +286,10 @@ struct AdjointState {
   double *ck = nullptr;    // nck checkpoints of u, v (stride each), 12 stresses
   double *tape = nullptr;  // tape entries: u then v, 2*stride doubles each
   int tape_entries = 0;
+  // Tape entries [0, ndte - n_cp] hold the taped tail (when n_cp < ndte);
+  // the sweep recomputes a checkpointed segment into interval + 1 entries
+  // from seg_base on, after the tail, so the tail survives for later sweeps.
+  int seg_base = 0;
   bool valid = false, uinit_explicit = false, seeded = false;
   int ndte = 0, interval = 0, nck = 0, n_cp = 0;
   long long budget = 0;  // bytes for checkpoints and tape (0: 80% of free memory)
@@ -534,8 +538,12 @@ int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
   // split of the subcycles into a checkpointed head and a taped tail
   int k = 0, n_cp = 0;
   if (interval > 0) {
+    // checkpoints every k subcycles, except for the last segment: the
+    // recording tapes its velocities (the tape holds a segment anyway), so
+    // the sweep reverses it without recomputing it
     k = std::min(interval, ndte);
-    n_cp = ndte;
+    n_cp = k * ((ndte - 1) / k);
+    if (n_cp == 0) k = 0;
   } else {
     size_t freeb = 0, totalb = 0;
     ADJ_TRY(cudaMemGetInfo(&freeb, &totalb));
@@ -546,19 +554,24 @@ int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
       // a checkpoints-only recording; the rest of the budget tapes the tail
       k = (int)std::ceil(std::sqrt((double)ndte * (double)ckpt / (double)entry));
       k = std::max(1, std::min(k, ndte));
+      // the segment recompute needs k + 1 entries of its own; what is left
+      // of the budget tapes the final subcycles (a tail of T needs T + 1)
       const double nck_max = std::ceil((double)ndte / k);
-      double entries = std::floor((budget - nck_max * (double)ckpt) / (double)entry);
-      entries = std::max(entries, (double)(k + 1));
-      n_cp = std::max(0, ndte - ((int)std::min(entries, (double)(ndte + 1)) - 1));
+      const double left =
+          std::floor((budget - nck_max * (double)ckpt) / (double)entry) - (double)(k + 1);
+      const int tail = left >= 2.0 ? (int)std::min(left - 1.0, (double)ndte) : 0;
+      n_cp = ndte - tail;
       if (n_cp == 0) k = 0;
     }
   }
   const int nck = n_cp > 0 ? (n_cp + k - 1) / k : 0;
-  const int entries = std::max(ndte - n_cp + 1, n_cp > 0 ? k + 1 : 0);
+  const int tail_entries = n_cp < ndte ? ndte - n_cp + 1 : 0;
+  const int entries = tail_entries + (n_cp > 0 ? k + 1 : 0);
   ADJ_CHECK(ensure_store(A, (size_t)nck * ckpt + (size_t)entries * entry));
   A.ck = (double *)A.store;
   A.tape = A.ck + (size_t)nck * (ckpt / sizeof(double));
   A.tape_entries = entries;
+  A.seg_base = tail_entries;
   A.interval = k;
   A.nck = nck;
   A.n_cp = n_cp;
@@ -698,22 +711,24 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
   const int k = A.interval;
   for (int j = A.nck - 1; j >= 0; j--) {
     const int len = std::min(k, A.n_cp - j * k);
-    ADJ_TRY(cudaMemcpyAsync(tape_u(A, 0), ck_u(A, j), sizeof(double) * d.nuv,
+    ADJ_TRY(cudaMemcpyAsync(tape_u(A, A.seg_base), ck_u(A, j), sizeof(double) * d.nuv,
                             cudaMemcpyDeviceToDevice, st));
-    ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), ck_v(A, j), sizeof(double) * d.nuv,
+    ADJ_TRY(cudaMemcpyAsync(tape_v(A, A.seg_base), ck_v(A, j), sizeof(double) * d.nuv,
                             cudaMemcpyDeviceToDevice, st));
     for (int q = 0; q < 12; q++)
       ADJ_TRY(cudaMemcpyAsync(A.spp[0][q], ck_s(A, j, q), sizeof(double) * d.nslots,
                               cudaMemcpyDeviceToDevice, st));
     // recompute the segment's velocities from its checkpoint
+    const int e0 = A.seg_base;
     for (int i = 0; i < len; i++) {
       const int b = i & 1;
-      launch_state(h, A.spp[b], A.spp[1 - b], tape_u(A, i), tape_v(A, i), tape_u(A, i + 1),
-                   tape_v(A, i + 1), false);
+      launch_state(h, A.spp[b], A.spp[1 - b], tape_u(A, e0 + i), tape_v(A, e0 + i),
+                   tape_u(A, e0 + i + 1), tape_v(A, e0 + i + 1), false);
       launches++;
     }
     for (int i = len - 1; i >= 0; i--)
-      reverse_step(tape_u(A, i), tape_v(A, i), tape_u(A, i + 1), tape_v(A, i + 1));
+      reverse_step(tape_u(A, e0 + i), tape_v(A, e0 + i), tape_u(A, e0 + i + 1),
+                   tape_v(A, e0 + i + 1));
   }
   if (one)
     k_adj_final<true><<<grid, kThreads, 0, st>>>(a, A.uinit_explicit ? 0 : 1);

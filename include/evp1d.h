@@ -266,9 +266,11 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
  *
  * 1. evp1d_run_checkpointed: the same call as evp1d_run, recording what the
  *    reverse sweep needs on the device:
- *      interval > 0:  (u, v, 12 stresses) every `interval` subcycles; the
- *                     sweep recomputes each segment's velocities from its
- *                     checkpoint (one extra forward in all);
+ *      interval > 0:  (u, v, 12 stresses) at the start of every
+ *                     `interval` subcycles, except that the velocities of
+ *                     the last segment are taped; the sweep recomputes each
+ *                     checkpointed segment's velocities from its checkpoint
+ *                     (one extra forward, less the last segment);
  *      interval <= 0: sized to device memory (the budget of
  *                     evp1d_set_adjoint_budget, default 80% of the free
  *                     memory): every subcycle's velocities when they fit (no

@@ -50,7 +50,10 @@ def test_adjoint_matches_tape(oracle_mod, curvilinear, interval):
     p = evp1d.set_evp_parameters(ndte)
     g, fs, info = gpu_grads(pr, ndte, uobs, vobs, interval=interval, stress=True)
     assert info["valid"] == 1
-    assert info["tape_subcycles"] == (ndte if interval == 0 else 0)
+    # interval mode tapes the last segment; the rest is checkpointed
+    k = min(interval, ndte)
+    assert info["tape_subcycles"] == (ndte if interval == 0 else ndte - k * ((ndte - 1) // k))
+    assert info["checkpoints"] == (0 if interval == 0 else (ndte - 1) // k)
     t = evp_tape.gradient(pr, ndte, p, uobs, vobs)
     for k in FIELDS:
         assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
@@ -81,7 +84,8 @@ def test_checkpoint_and_tape_sweeps_agree_bitwise():
     ga, _, ia = gpu_grads(pr, pr.ndte, uobs, vobs, interval=0)
     for interval in (1, 7, 31, 100):
         gb, _, ib = gpu_grads(pr, pr.ndte, uobs, vobs, interval=interval)
-        assert ib["checkpoints"] == -(-pr.ndte // min(interval, pr.ndte))
+        # every interval but the last segment, which is taped
+        assert ib["checkpoints"] == (pr.ndte - 1) // min(interval, pr.ndte)
         for k in ga:
             assert np.array_equal(ga[k].view(np.int64), gb[k].view(np.int64)), (interval, k)
 
@@ -117,26 +121,37 @@ def test_recordings_on_one_handle_and_constant_slots(oracle_mod):
 
 
 def test_memory_sized_recording_with_a_small_budget():
-    """A budget of 45 velocity-tape entries (of 61): the first subcycles are
-    checkpointed and recomputed, the final ones taped; the forward outputs
-    and the gradients are those of the full tape, bit for bit."""
+    """A budget halfway between the least a recording needs (checkpoints at
+    the memory-minimising interval plus one segment of recompute space) and
+    the full tape: the first subcycles are checkpointed and recomputed, the
+    final ones taped; the forward outputs and the gradients are those of the
+    full tape, bit for bit, and a second sweep of the same recording (whose
+    segment recompute must not overwrite the taped tail) gives them again."""
     pr = small(seed=46, ndte=60)
     uobs, vobs = synth.observations(pr.na, seed=4)
     ga, fa, ia = gpu_grads(pr, pr.ndte, uobs, vobs, interval=0)
     assert ia["tape_subcycles"] == pr.ndte
-    entry = ia["store_bytes"] // (pr.ndte + 1)
+    full = ia["store_bytes"]
+    with evp1d.EVP1D.from_problem(pr) as s:
+        s.set_adjoint_budget(1)  # below the minimum: gets the minimum
+        s.run_checkpointed(pr.ndte, evp1d.FieldSet.from_problem(pr), 0)
+        least = s.adjoint_info()
+    assert least["tape_subcycles"] == 0 and least["checkpoints"] > 0, least
+    budget = (least["store_bytes"] + full) // 2
     fs = evp1d.FieldSet.from_problem(pr)
     with evp1d.EVP1D.from_problem(pr) as s:
-        s.set_adjoint_budget(entry * 45)
+        s.set_adjoint_budget(budget)
         s.run_checkpointed(pr.ndte, fs, 0)
         info = s.adjoint_info()
         g = s.adjoint(2 * (fs.uvel[: pr.na] - uobs), 2 * (fs.vvel[: pr.na] - vobs))
+        g2 = s.adjoint(2 * (fs.uvel[: pr.na] - uobs), 2 * (fs.vvel[: pr.na] - vobs))
     assert 0 < info["tape_subcycles"] < pr.ndte and info["checkpoints"] > 0, info
-    assert info["store_bytes"] <= entry * 45
+    assert info["store_bytes"] <= budget
     for a, b in ((fs.uvel, fa.uvel), (fs.vvel, fa.vvel), (fs.stress, fa.stress)):
         assert np.array_equal(a.view(np.int64), b.view(np.int64))
     for k in ga:
         assert np.array_equal(ga[k].view(np.int64), g[k].view(np.int64)), k
+        assert np.array_equal(g2[k].view(np.int64), g[k].view(np.int64)), k
 
 
 def central_difference(run, pr, field, d, h, uobs, vobs):
