@@ -106,8 +106,8 @@ int check_device_error(evp1d_t *h) {
   CHECK(evp::problem_take_error(&h->d, &code));
   if (code)
     return fail(EVP1D_ERR_TIMEOUT,
-                "a bounded device wait ran out (code %d: 1 consumer, 2 producer, "
-                "3 drain); the results of this call are not valid", code);
+                "a bounded device-side wait ran out (code %d: %s); the results of this "
+                "call are not valid", code, evp::tma_wait_name(code));
   return EVP1D_OK;
 }
 
@@ -506,6 +506,16 @@ int evp1d_synchronize(evp1d_t *h) {
   CHECK(select_device(h));
   CUDA_TRY(cudaStreamSynchronize(h->d.stream));
   return check_device_error(h);
+}
+
+int evp1d_debug_wait_timeout(evp1d_t *h, long long ns) {
+  if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
+  if (ns < 1000000 || ns > 1000000000)
+    return fail(EVP1D_ERR_INVALID_ARG, "wait limit %lld ns outside [1e6, 1e9]", ns);
+  CUDA_TRY(cudaSetDevice(h->d.device));
+  evp::launch_wait_probe(h->d.err, (unsigned long long)ns, h->d.stream);
+  CUDA_TRY(cudaGetLastError());
+  return EVP1D_OK;
 }
 
 int evp1d_debug_trace(evp1d_t *h, long long *out, int n) {

@@ -754,7 +754,8 @@ int evp1d_adjoint_gradients(evp1d_t *h, const evp1d_grads *g) {
   ADJ_CHECK(problem_take_error(&d, &code));
   if (code)
     return error(EVP1D_ERR_TIMEOUT,
-                 "a bounded device wait ran out (code %d); the gradients are not valid", code);
+                 "a bounded device-side wait ran out (code %d: %s); the gradients are not valid",
+                 code, tma_wait_name(code));
   const size_t nv = (size_t)(d.navel > 0 ? d.navel : 1);
   const size_t bn = sizeof(double) * (size_t)d.na;
   struct Out {

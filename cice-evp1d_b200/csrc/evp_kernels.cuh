@@ -116,6 +116,11 @@ constexpr int kTraceTiles = 256;
 
 // Allow the kernel's dynamic shared memory (call once per device).
 int tma_prepare(int device);
+// What the wait that left `code` in the error word was waiting for.
+const char *tma_wait_name(int code);
+// One bounded wait on an mbarrier that nothing completes: it runs out after
+// limit_ns and leaves its code in *err (a check of the timeout path).
+void launch_wait_probe(int *err, unsigned long long limit_ns, cudaStream_t st);
 void launch_tma(const TmaArgs &a, const Params &p, bool last, int nctas,
                 cudaStream_t st);
 

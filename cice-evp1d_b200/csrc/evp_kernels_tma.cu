@@ -128,13 +128,15 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Bounded wait for the phase of parity `parity` to complete.
+// Bounded wait for the phase of parity `parity` to complete; on expiry the
+// wait's code goes into the error word.
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity,
-                                          int *err, int code) {
+                                          int *err, int code,
+                                          unsigned long long limit_ns = kWaitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > kWaitNs) {
+    if (global_ns() - t0 > limit_ns) {
       atomicMax(err, code);
       return false;
     }
@@ -559,7 +561,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
 
 size_t smem_bytes() { return sizeof(Smem); }
 
+// One thread waits, through the kernel's own bounded wait, on an mbarrier at
+// which nothing ever arrives: the wait runs out after limit_ns and records
+// kProbeCode, as a timed-out wait of the subcycle kernel would.
+constexpr int kProbeCode = 12;
+
+__global__ void k_wait_probe(int *err, unsigned long long limit_ns) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    mbar_wait(&bar, 0, err, kProbeCode, limit_ns);
+  }
+}
+
 }  // namespace
+
+const char *tma_wait_name(int code) {
+  switch (code) {
+    case 1: return "a consumer waited for a tile's stress inputs";
+    case 2: return "the producer waited for a free stress slot";
+    case 3: return "the producer waited for its copies to land after an early stop";
+    case 6: return "the producer waited for a tile record";
+    case 7: return "the producer waited for records issued ahead";
+    case 8: return "the dynamic shared memory was not 16-byte aligned";
+    case 9: return "the producer waited for the stepu slot";
+    case 10: return "the producer waited for its last stepu copy";
+    case 11: return "a consumer waited for a tile's stepu inputs";
+    case kProbeCode: return "the wait probe (evp1d_debug_wait_timeout)";
+    default: return "unknown";
+  }
+}
+
+void launch_wait_probe(int *err, unsigned long long limit_ns, cudaStream_t st) {
+  k_wait_probe<<<1, 32, 0, st>>>(err, limit_ns);
+}
 
 int tma_prepare(int device) {
   const int bytes = (int)smem_bytes();

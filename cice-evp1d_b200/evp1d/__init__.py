@@ -361,6 +361,11 @@ class EVP1D:
     def synchronize(self) -> None:
         check(self._L.evp1d_synchronize(self.h), "evp1d_synchronize")
 
+    def debug_wait_timeout(self, ns: int) -> None:
+        """Queue one bounded wait that runs out after ns nanoseconds
+        (evp1d_debug_wait_timeout): the next synchronize raises the timeout."""
+        check(self._L.evp1d_debug_wait_timeout(self.h, int(ns)), "evp1d_debug_wait_timeout")
+
     @property
     def path(self) -> str:
         """Name of the kernel path the library runs."""

@@ -162,6 +162,14 @@ int evp1d_stepu_only(evp1d_t *handle, int n);
  * device-side wait of the solver ran out since the last check. */
 int evp1d_synchronize(evp1d_t *handle);
 
+/* Debug: a check of the timeout path; no counterpart in the reference.
+ * Queues on the handle's stream one wait of the solver's own bounded kind on
+ * a barrier that nothing completes, limited to `ns` nanoseconds (1e6 to 1e9).
+ * It runs out and leaves its code in the handle's error word, so the next
+ * evp1d_synchronize (or call that checks the word) returns EVP1D_ERR_TIMEOUT
+ * and clears it; the handle stays usable. */
+int evp1d_debug_wait_timeout(evp1d_t *handle, long long ns);
+
 /* Debug: timing trace of the TMA kernel's block 0 in the last launch
  * (recorded only when EVP1D_TRACE is set at evp1d_init).  Up to 256 tiles x 8
  * %globaltimer stamps (ns): [0] the producer warps issued all of the tile's
