@@ -644,10 +644,11 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
   }
   evp::TilePlan plan;
   evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan);
-  long long hmax = 0, tmax = 0;
+  long long hmax = 0, tmax = 0, xmax = 0;
   for (int t = 0; t < plan.ntiles; t++) {
     if (plan.halo_cnt[t] > hmax) hmax = plan.halo_cnt[t];
     if (plan.tile_cnt[t] > tmax) tmax = plan.tile_cnt[t];
+    if (plan.uvx_cnt[t] > xmax) xmax = plan.uvx_cnt[t];
   }
   for (int k = 0; k < 8; k++) stats[k] = 0;
   stats[0] = plan.ntiles;
@@ -656,6 +657,7 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
   stats[3] = plan.from_coords ? 1 : 0;
   stats[4] = hmax;
   stats[5] = tmax;
+  stats[6] = xmax;
   return EVP1D_OK;
 }
 

@@ -262,7 +262,9 @@ int evp1d_dyn_sizes(evp1d_dyn_t *handle, int *na, int *navel);
  * stats[0] tiles, [1] device slots (list points + alignment padding),
  * [2] forward-halo points summed over tiles, [3] 1 if the tiles follow grid
  * coordinates rebuilt from the neighbour vectors (0: consecutive list points),
- * [4] largest halo of one tile, [5] largest tile.
+ * [4] largest halo of one tile, [5] largest tile, [6] largest number of
+ * extra velocity points (read by the stencil, owned by no tile point) of one
+ * tile.
  * -------------------------------------------------------------------------- */
 int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
                      const int32_t *se, const int32_t *nw, const int32_t *sw,

@@ -123,3 +123,16 @@ def random_graph_problem(na: int, nhalo: int, seed: int) -> synth.Problem1D:
                            skipU=skipU, f=f, stress=np.zeros((12, na)),
                            uvel=uvel, vvel=vvel, strintx=np.zeros(na),
                            strinty=np.zeros(na), Cb=np.zeros(na))
+
+
+def halo_limited_problem(na: int, nhalo: int, seed: int, nshared: int = 2) -> synth.Problem1D:
+    """A random-graph problem whose stress neighbours (ee, ne, se) all point at
+    `nshared` slots while the stepu neighbours (nw, sw, sse) stay random: each
+    point brings three new forward-halo points but almost no extra velocities,
+    so the tile plan cuts its tiles at the forward-halo cap (64 points)."""
+    pr = random_graph_problem(na, nhalo, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shared = rng.integers(1, pr.navel + 1, nshared).astype(np.int32)
+    for k in ("ee", "ne", "se"):
+        pr.idx[k] = rng.choice(shared, pr.na).astype(np.int32)
+    return pr

@@ -204,6 +204,14 @@ def test_shuffled_list_order(oracle_mod):
     assert_same(gpu_run(pr, 9), oracle_run(oracle_mod, pr, 9), pr)
 
 
+def test_tiles_at_the_halo_cap(oracle_mod):
+    """Tiles cut at the forward-halo cap: 64 recomputed halo points fill both
+    halo warps and the halo arrays of a stage."""
+    pr = helpers.halo_limited_problem(3000, 50, 7)
+    assert evp1d.plan_stats(pr.na, pr.navel, pr.idx)["max_halo"] == 64
+    assert_same(gpu_run(pr, pr.ndte), oracle_run(oracle_mod, pr, pr.ndte), pr)
+
+
 @pytest.mark.parametrize("na,nhalo,seed", [(5000, 300, 0), (777, 5, 1)])
 def test_irregular_graph(oracle_mod, na, nhalo, seed):
     """Random neighbour slots (no grid): consecutive-point tiles whose halo

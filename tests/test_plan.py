@@ -52,3 +52,16 @@ def test_empty_plan():
     z = np.zeros(0, np.int32)
     s = evp1d.plan_stats(0, 0, {k: z for k in ("ee", "ne", "se", "nw", "sw", "sse")})
     assert s["tiles"] == 0 and s["slots"] == 0
+
+
+def test_caps_are_reached_and_kept():
+    """The two per-tile caps of the TMA kernel's shared-memory arrays: the
+    forward halo (64 points) binds for a graph whose stress neighbours are a
+    few shared slots, the extra velocities (128) for a random graph and for
+    a grid; neither is exceeded."""
+    pr = helpers.halo_limited_problem(3000, 50, 7)
+    s = evp1d.plan_stats(pr.na, pr.navel, pr.idx)
+    assert s["max_halo"] == 64 and s["max_extras"] <= 128, s
+    pr = helpers.random_graph_problem(5000, 300, 0)
+    s = evp1d.plan_stats(pr.na, pr.navel, pr.idx)
+    assert s["max_extras"] == 128 and s["max_halo"] <= 64, s
