@@ -132,7 +132,7 @@ __device__ __forceinline__ void str_lam(const AdjArgs &a, int t, int w, double &
 }
 
 template <bool kOne>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)  // 64 registers: 32 warps per SM
 k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__restrict__ v0,
             const double *__restrict__ u1, const double *__restrict__ v1) {
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.nslots;

@@ -121,45 +121,56 @@ __host__ __device__ __forceinline__ void corner_adjoint(
   }
 }
 
-// Transpose of strain_rates (src/bench_v2b.F90:363-395): lam of the corner
-// velocities from lam of div, ten, shr at the corners ne, nw, sw, se.
-// out[0..7] = lam of ucc, vcc, uee, vee, une, vne, use, vse.
-__host__ __device__ __forceinline__ void strain_adjoint(const double (&D)[4],
-                                                        const double (&T)[4],
-                                                        const double (&H)[4],
-                                                        const Geom &g, double (&out)[8]) {
-  const double dxT = g.dxT, dyT = g.dyT, cxp = g.cxp, cyp = g.cyp, cxm = g.cxm, cym = g.cym;
-  out[0] = cyp * D[0] + dyT * D[1] - cym * T[0] + dyT * T[1] - cxm * H[0] + dxT * H[3];
-  out[1] = cxp * D[0] + dxT * D[3] + cxm * T[0] - dxT * T[3] - cym * H[0] + dyT * H[1];
-  out[2] = -dyT * D[0] + cym * D[1] - dyT * T[0] - cyp * T[1] - cxm * H[1] + dxT * H[2];
-  out[3] = cxp * D[1] + dxT * D[2] + cxm * T[1] - dxT * T[2] - dyT * H[0] - cyp * H[1];
-  out[4] = cym * D[2] - dyT * D[3] - cyp * T[2] - dyT * T[3] - dxT * H[1] - cxp * H[2];
-  out[5] = -dxT * D[1] + cxm * D[2] + dxT * T[1] + cxp * T[2] - cyp * H[2] - dyT * H[3];
-  out[6] = dyT * D[2] + cyp * D[3] + dyT * T[2] - cym * T[3] - dxT * H[0] - cxp * H[3];
-  out[7] = -dxT * D[0] + cxm * D[3] + dxT * T[0] + cxp * T[3] + dyT * H[2] - cym * H[3];
-}
-
 // Reverse of stress at one T point.  lo = lam of str1..str8 written by the
 // subcycle, ls = lam of the updated stresses (in: from later subcycles; out:
 // lam of the old stresses).  Returns the lam of the 8 corner velocities and
 // the point's dJ/dstrength contribution.
+//
+// Corner by corner: corner_strain gives the corner's div, ten, shr and Delta
+// (bit for bit those of strain_rates, so every branch follows the forward),
+// corner_adjoint reverses its relaxation, and the corner's share of the
+// transposed strain rates is added to lc at once.  Only one corner's strain
+// is live at a time.  With P1 = (cc, ee, ne, se)[k], P2 = (ee, cc, se, ne)[k],
+// P4 = (se, ne, ee, cc)[k] and the coefficients of corner_strain:
+//   lam u[P1] += A1 D - C1 T - C3 H,  lam v[P1] += A3 D + C3 T - C1 H,
+//   lam u[P2] += B2 (D + T),          lam v[P2] += B2 H,
+//   lam u[P4] += B4 H,                lam v[P4] += B4 (D - T).
 __host__ __device__ __forceinline__ void stress_adjoint(const Corners &c, const Geom &g,
                                                         double strength, const Params &p,
                                                         const double (&lo)[8],
                                                         double (&ls)[12], double (&lc)[8],
                                                         double &l_strength) {
   str_combine_adjoint(lo, g, ls);
-  const Strain sr = strain_rates(c, g, p.e_factor);
-  double D[4], T[4], H[4];
+  const double uu[4] = {c.ucc, c.uee, c.une, c.use};
+  const double vv[4] = {c.vcc, c.vee, c.vne, c.vse};
+#pragma unroll
+  for (int q = 0; q < 8; q++) lc[q] = 0.0;
   l_strength = 0.0;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    double lst;
-    corner_adjoint(ls[k], ls[4 + k], ls[8 + k], sr.div[k], sr.ten[k], sr.shr[k],
-                   sr.Delta[k], strength, g.DminTarea, p, D[k], T[k], H[k], lst);
+    const int p1 = k, p2 = k ^ 1, p4 = 3 - k;
+    double div, ten, shr, Delta;
+    corner_strain(k, uu[p1], vv[p1], uu[p2], vv[p2], uu[p4], vv[p4], g, p.e_factor, div, ten,
+                  shr, Delta);
+    double D, T, H, lst;
+    corner_adjoint(ls[k], ls[4 + k], ls[8 + k], div, ten, shr, Delta, strength, g.DminTarea, p,
+                   D, T, H, lst);
     l_strength += lst;
+    const bool a = (k == 0) | (k == 3);
+    const bool b = k < 2;
+    const double A1 = a ? g.cyp : g.cym;
+    const double C1 = a ? g.cym : g.cyp;
+    const double A3 = b ? g.cxp : g.cxm;
+    const double C3 = b ? g.cxm : g.cxp;
+    const double B2 = a ? -g.dyT : g.dyT;
+    const double B4 = b ? -g.dxT : g.dxT;
+    lc[2 * p1] += A1 * D - C1 * T - C3 * H;
+    lc[2 * p1 + 1] += A3 * D + C3 * T - C1 * H;
+    lc[2 * p2] += B2 * (D + T);
+    lc[2 * p2 + 1] += B2 * H;
+    lc[2 * p4] += B4 * H;
+    lc[2 * p4 + 1] += B4 * (D - T);
   }
-  strain_adjoint(D, T, H, g, lc);
 }
 
 // Reverse of stepu at one U point (src/bench_v2b.F90:509-544) from the
