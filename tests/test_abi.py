@@ -133,3 +133,29 @@ def test_native_index_build_capacity_error(lib):
     rc = lib.evp1d_build_index(6, 6, 1, m.ctypes.data_as(P), 3, 3, C.byref(na),
                                C.byref(navel), *[small.ctypes.data_as(P)] * 9)
     assert rc == -1 and na.value == 25 and navel.value > 25
+
+
+def test_header_compiles_as_c_and_layouts_match_bindings(lib, tmp_path):
+    """A C99 caller of include/evp1d.h sees the struct layouts the Python
+    binding uses, and host-only calls work from C."""
+    import ctypes
+    from evp1d import _lib
+    from evp1d.dyn import DynFields
+    exe = str(tmp_path / "abi_layout")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "native", "abi_layout.c"), "-o", exe,
+                    "-L", os.path.dirname(LIB), "-levp1d",
+                    "-Wl,-rpath," + os.path.dirname(LIB)], check=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    got = dict(line.rsplit(" ", 1) for line in out.strip().splitlines())
+    py = {"evp1d_params": _lib.Params, "evp1d_fields": _lib.Fields,
+          "evp1d_grads": _lib.Grads, "evp1d_dyn_fields": DynFields}
+    for key, val in got.items():
+        if "." in key:
+            t, m = key.split(".")
+            assert getattr(py[t], m).offset == int(val), key
+        elif key in py:
+            assert ctypes.sizeof(py[key]) == int(val), key
+    assert got["brlx"] == "120.0"
+    assert got["run_null"] == "-1,1"  # EVP1D_ERR_INVALID_ARG and a message
+    assert got["version"] == "1"
