@@ -13,7 +13,10 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__global__ void __launch_bounds__(kThreads)
+// At most 128 registers: two blocks (16 warps) per SM.  kStd: parameters
+// with std_params(p) (stress_update_std).
+template <bool kStd>
+__global__ void __launch_bounds__(kThreads, 2)
 k_stress_ref(DevState s, Params p) {
   const int n = s.na;
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < n;
@@ -35,7 +38,10 @@ k_stress_ref(DevState s, Params p) {
     double st[12], out[8];
 #pragma unroll
     for (int k = 0; k < 12; k++) st[k] = s.stress[k][w];
-    stress_update(st, out, sr, s.strength[w], g, p);
+    if (kStd)
+      stress_update_std(st, out, sr, s.strength[w], g, p);
+    else
+      stress_update(st, out, sr, s.strength[w], g, p);
 #pragma unroll
     for (int k = 0; k < 12; k++) s.stress[k][w] = st[k];
 #pragma unroll
@@ -92,7 +98,10 @@ int grid_for(int n) {
 
 void launch_stress(const DevState &s, const Params &p, cudaStream_t st) {
   if (s.na <= 0) return;
-  k_stress_ref<<<grid_for(s.na), kThreads, 0, st>>>(s, p);
+  if (std_params(p))
+    k_stress_ref<true><<<grid_for(s.na), kThreads, 0, st>>>(s, p);
+  else
+    k_stress_ref<false><<<grid_for(s.na), kThreads, 0, st>>>(s, p);
 }
 
 void launch_stepu(const DevState &s, const Params &p, cudaStream_t st) {
