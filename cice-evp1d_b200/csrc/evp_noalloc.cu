@@ -62,7 +62,8 @@ __global__ void __launch_bounds__(kThreads) k_na_check(NaArgs a, int *status) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_na_stress(NaArgs a, Params p) {
+// At most 128 registers: two blocks (16 warps) per SM.
+__global__ void __launch_bounds__(kThreads, 2) k_na_stress(NaArgs a, Params p) {
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < a.na;
        w += gridDim.x * blockDim.x) {
     if (a.skipT[w]) continue;
