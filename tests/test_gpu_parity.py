@@ -283,6 +283,23 @@ def test_shortcut_edges(oracle_mod, u0):
     assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 7, params=p), pr)
 
 
+def test_nonfinite_inputs(oracle_mod):
+    """Non-finite and extreme inputs take the straight-line stress's fallback
+    (NaN strain rates, strength at or above 1e300*DminArea) and propagate as
+    the reference does: NaN velocities at some points, infinite and huge
+    strength at others; NaNs are compared by position."""
+    pr = synth.make_problem("grid400x300", nx=60, ny=44, seed=17, ndte=5)
+    rng = np.random.default_rng(21)
+    n = pr.na
+    pick = lambda f: rng.random(n) < f
+    pr.uvel[:n] = np.where(pick(0.01), np.nan, pr.uvel[:n])
+    pr.vvel[:n] = np.where(pick(0.01), np.inf, pr.vvel[:n])
+    pr.f["uvel_init"], pr.f["vvel_init"] = pr.uvel[:n].copy(), pr.vvel[:n].copy()
+    pr.f["strength"] = np.where(pick(0.01), np.inf, np.where(pick(0.01), 1e305, pr.f["strength"]))
+    fs = gpu_run(pr, 5)
+    assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 5), pr)
+
+
 def test_golden_fixture_md5():
     """The CUDA path reproduces the committed fixture's md5s and arrays."""
     import golden_io
