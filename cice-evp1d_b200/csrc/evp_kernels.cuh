@@ -71,9 +71,10 @@ void launch_fused(const FusedArgs &a, const Params &p, bool last,
 
 // The same subcycle as a persistent producer/consumer kernel fed by TMA bulk
 // copies (evp_kernels_tma.cu).  sf = 7 stress inputs (dxT, dyT, HTE, HTN,
-// HTEm1, HTNm1, strength) then the 12 input stresses; uf = 13 stepu inputs
-// (kvrel, uocn, vocn, waterx, watery, forcex, forcey, umassdti, fm, uarear,
-// Tbu, uinit, vinit).
+// HTEm1, HTNm1, strength) then the 12 input stresses, read by the halo
+// gathers and the stress copies; the 13 stepu inputs (kvrel, uocn, vocn,
+// waterx, watery, forcex, forcey, umassdti, fm, uarear, Tbu, uinit, vinit)
+// come from the constant blocks.
 constexpr int kTmaStressFields = 19;
 constexpr int kTmaStepuFields = 13;
 // Per-call constants of a tile in one contiguous block: kConstFields x
@@ -96,7 +97,6 @@ struct TmaArgs {
   // per tile one producer record of kRecInts int32 (evp_tiles.h)
   const int32_t *tile_rec = nullptr;
   const double *sf[kTmaStressFields] = {};
-  const double *uf[kTmaStepuFields] = {};
   const double *cblk = nullptr;  // constant blocks, kConstFields x kTileOwned per tile
   const double *u_in = nullptr, *v_in = nullptr;
   double *u_out = nullptr, *v_out = nullptr;

@@ -472,11 +472,6 @@ TmaArgs problem_tma_args(const DeviceProblem &d, int from) {
   for (int k = 0; k < 6; k++) a.sf[k] = d.geo[geo_order[k]];
   a.sf[6] = d.dyn[kStrength];
   for (int k = 0; k < 12; k++) a.sf[7 + k] = d.stress[from][k];
-  const int uf_order[kTmaStepuFields] = {kKvrel, kUocn, kVocn, kWaterx, kWatery,
-                                         kForcex, kForcey, kUmassdti, kFm, -1,
-                                         kTbu, kUinit, kVinit};
-  for (int k = 0; k < kTmaStepuFields; k++)
-    a.uf[k] = uf_order[k] < 0 ? d.geo[kUarear] : d.dyn[uf_order[k]];
   a.cblk = d.cblk;
   a.u_in = d.u[from];
   a.v_in = d.v[from];
