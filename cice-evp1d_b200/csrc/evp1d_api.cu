@@ -412,6 +412,7 @@ int evp1d_set_params(evp1d_t *h, const evp1d_params *params) {
 }
 
 int evp1d_upload(evp1d_t *h, const evp1d_fields *io) {
+  evp::NvtxRange nvtx_range("evp1d_upload");
   if (!h || !io) return fail(EVP1D_ERR_INVALID_ARG, "NULL argument");
   CHECK(select_device(h));
   evp::adjoint_invalidate(h->adj);
@@ -428,6 +429,7 @@ int evp1d_upload(evp1d_t *h, const evp1d_fields *io) {
 }
 
 int evp1d_subcycles(evp1d_t *h, int ndte) {
+  evp::NvtxRange nvtx_range("evp1d_subcycles");
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (ndte < 0) return fail(EVP1D_ERR_INVALID_ARG, "ndte = %d < 0", ndte);
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");
@@ -455,6 +457,7 @@ int evp1d_subcycles(evp1d_t *h, int ndte) {
 }
 
 int evp1d_download(evp1d_t *h, const evp1d_fields *io) {
+  evp::NvtxRange nvtx_range("evp1d_download");
   if (!h || !io) return fail(EVP1D_ERR_INVALID_ARG, "NULL argument");
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "nothing uploaded");
   CHECK(select_device(h));
@@ -470,12 +473,14 @@ int evp1d_download(evp1d_t *h, const evp1d_fields *io) {
 }
 
 int evp1d_run(evp1d_t *h, int ndte, const evp1d_fields *io) {
+  evp::NvtxRange nvtx_range("evp1d_run");
   CHECK(evp1d_upload(h, io));
   CHECK(evp1d_subcycles(h, ndte));
   return evp1d_download(h, io);
 }
 
 int evp1d_stress_only(evp1d_t *h, int n) {
+  evp::NvtxRange nvtx_range("evp1d_stress_only");
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (n < 0) return fail(EVP1D_ERR_INVALID_ARG, "n = %d < 0", n);
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");
@@ -489,6 +494,7 @@ int evp1d_stress_only(evp1d_t *h, int n) {
 }
 
 int evp1d_stepu_only(evp1d_t *h, int n) {
+  evp::NvtxRange nvtx_range("evp1d_stepu_only");
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (n < 0) return fail(EVP1D_ERR_INVALID_ARG, "n = %d < 0", n);
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");

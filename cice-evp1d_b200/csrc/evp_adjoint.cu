@@ -512,6 +512,7 @@ using namespace evp;
 extern "C" {
 
 int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
+  evp::NvtxRange nvtx_range("evp1d_record_subcycles");
   if (!h) return error(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (ndte < 1) return error(EVP1D_ERR_INVALID_ARG, "ndte = %d < 1", ndte);
   if (!h->uploaded) return error(EVP1D_ERR_STATE, "evp1d_upload has not been called");
@@ -635,6 +636,7 @@ int evp1d_run_checkpointed(evp1d_t *h, int ndte, const evp1d_fields *io, int int
 
 int evp1d_adjoint_seed(evp1d_t *h, const double *lam_uvel, const double *lam_vvel,
                        const double *const *lam_stress) {
+  evp::NvtxRange nvtx_range("evp1d_adjoint_seed");
   if (!h) return error(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (!h->adj || !h->adj->valid)
     return error(EVP1D_ERR_STATE, "no recorded forward: call evp1d_run_checkpointed first");
@@ -677,6 +679,7 @@ int evp1d_adjoint_seed(evp1d_t *h, const double *lam_uvel, const double *lam_vve
 }
 
 int evp1d_adjoint_sweep(evp1d_t *h) {
+  evp::NvtxRange nvtx_range("evp1d_adjoint_sweep");
   if (!h) return error(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (!h->adj || !h->adj->valid)
     return error(EVP1D_ERR_STATE, "no recorded forward: call evp1d_run_checkpointed first");
@@ -742,6 +745,7 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
 }
 
 int evp1d_adjoint_gradients(evp1d_t *h, const evp1d_grads *g) {
+  evp::NvtxRange nvtx_range("evp1d_adjoint_gradients");
   if (!h || !g) return error(EVP1D_ERR_INVALID_ARG, "NULL argument");
   if (!h->adj || !h->adj->valid)
     return error(EVP1D_ERR_STATE, "no recorded forward: call evp1d_run_checkpointed first");

@@ -176,6 +176,7 @@ int evp1d_dyn_init(evp1d_dyn_t **handle, int nx, int ny, int nghost,
 }
 
 int evp1d_dyn_run(evp1d_dyn_t *d, int ndte, const evp1d_dyn_fields *io) {
+  evp::NvtxRange nvtx_range("evp1d_dyn_run");
   if (!d || !io) return evp::error(EVP1D_ERR_INVALID_ARG, "NULL argument");
   const double *in[kIn2d] = {io->strength, io->cdn_ocn, io->aiu, io->uocn, io->vocn,
                              io->waterxU, io->wateryU, io->forcexU, io->forceyU,

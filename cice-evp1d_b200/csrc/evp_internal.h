@@ -6,6 +6,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "evp1d.h"
 #include "evp_kernels.cuh"
@@ -15,6 +16,15 @@ namespace evp {
 
 // Record `fmt` as this thread's last error message and return `code`.
 int error(int code, const char *fmt, ...);
+
+// A named NVTX range over a scope, so that the public calls show on a
+// profiler's timeline (header-only NVTX; without a profiler it does nothing).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Per-call input fields in the order they are staged and scattered.
 enum DynField {

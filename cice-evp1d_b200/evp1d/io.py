@@ -14,8 +14,9 @@ record markers), so that cases prepared for the Fortran benchmark run here:
   src/vars.F90:2233-2304 (writeout_1d): the 12 stresses [na each]; then
   strintx, strinty, uvel, vvel compacted over the points that are not skipU.
 
-``python -m evp1d.io <dir> [--ndte N] [--id b200]`` runs a case directory on
-the GPU the way src/evp_v2b.F90:57-123 does and writes its two output files.
+``python -m evp1d.io <dir> [--ndte N] [--id b200] [--stats]`` runs a case
+directory on the GPU the way src/evp_v2b.F90:57-123 does, writes its two
+output files and, with --stats, prints the reference's output statistics.
 """
 from __future__ import annotations
 
@@ -119,21 +120,48 @@ def write_outputs(path: str, ident: str, stress, strintx, strinty, uvel, vvel, s
     return hashlib.md5(a).hexdigest(), hashlib.md5(b).hexdigest()
 
 
+_STRESS_LABELS = ([f" stressp_{k}:" for k in range(1, 5)] + [f" stressm_{k}:" for k in range(1, 5)]
+                  + [f"stress12_{k}:" for k in range(1, 5)])
+
+
+def output_statistics(stress, strs, strintx, strinty, uvel, vvel) -> list:
+    """The lines of the reference's output statistics (stat_out_1d,
+    src/vars.F90:2209-2232): label, min, max and sum of the 12 stresses [na],
+    str1..str8 [navel] (when given), strintx, strinty [na] and uvel, vvel
+    [navel], in Fortran's a11,3f25.8 layout.  The sums are numpy's, whose
+    summation order is not Fortran's, so they agree to rounding only: a
+    diagnostic, not a bitwise check."""
+    def line(label, a):
+        a = np.asarray(a, dtype=np.float64)
+        return f"{label:>11}{a.min():25.8f}{a.max():25.8f}{a.sum():25.8f}"
+    out = [line(lab, stress[k]) for k, lab in enumerate(_STRESS_LABELS)]
+    if strs is not None:
+        out += [line(f"str{k + 1}:", strs[k]) for k in range(8)]
+    out += [line("strintx:", strintx), line("strinty:", strinty),
+            line("uvel:", uvel), line("vvel:", vvel)]
+    return out
+
+
 def run_case(path: str, na: int, navel: int, ndte: int, ident: str = "b200",
-             device: int = 0) -> tuple:
+             device: int = 0, stats: bool = False) -> tuple:
     """Read a case, run ndte subcycles on the GPU with set_evp_parameters(ndte)
     overridden by the file's four scalars (src/evp_v2b.F90:63, 68), write the
-    outputs, return their md5 sums."""
+    outputs, return their md5 sums (and, with stats, the output statistics
+    lines of output_statistics)."""
     import evp1d
     pr, scal = read_inputs(path, na, navel, ndte)
     p = evp1d.set_evp_parameters(ndte)
     for k, v in scal.items():
         setattr(p, k, v)
-    fs = evp1d.FieldSet.from_problem(pr, explicit_init=True)
+    fs = evp1d.FieldSet.from_problem(pr, explicit_init=True, want_str=stats)
     with evp1d.EVP1D.from_problem(pr, params=p, device=device) as s:
         s.run(ndte, fs)
-    return write_outputs(path, ident, fs.stress, fs.strintx, fs.strinty, fs.uvel,
+    sums = write_outputs(path, ident, fs.stress, fs.strintx, fs.strinty, fs.uvel,
                          fs.vvel, pr.skipU)
+    if not stats:
+        return sums
+    return sums + (output_statistics(fs.stress, fs.str, fs.strintx, fs.strinty,
+                                     fs.uvel, fs.vvel),)
 
 
 def main(argv=None):
@@ -143,9 +171,13 @@ def main(argv=None):
     ap.add_argument("--navel", type=int, required=True)
     ap.add_argument("--ndte", type=int, default=1)
     ap.add_argument("--id", default="b200")
+    ap.add_argument("--stats", action="store_true",
+                    help="print the reference's output statistics (stat_out_1d)")
     a = ap.parse_args(argv)
-    h1, h2 = run_case(a.dir, a.na, a.navel, a.ndte, a.id)
-    print(f"{h1}  output_stress_{a.id}_1d.bin\n{h2}  output_stepu_{a.id}_1d.bin")
+    res = run_case(a.dir, a.na, a.navel, a.ndte, a.id, stats=a.stats)
+    if a.stats:
+        print("\n".join(res[2]))
+    print(f"{res[0]}  output_stress_{a.id}_1d.bin\n{res[1]}  output_stepu_{a.id}_1d.bin")
 
 
 if __name__ == "__main__":
