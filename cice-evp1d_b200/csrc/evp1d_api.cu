@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <atomic>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -205,6 +206,10 @@ int check_device(int device) {
   return EVP1D_OK;
 }
 
+// Largest tile (points) of the plans of handles created from now on
+// (evp1d_set_tile_points).
+std::atomic<int> g_tile_points{evp::kTileOwned};
+
 // Validated 1-based neighbour vectors -> tile plan -> device problem.
 int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6],
                 const double *const geo[7], const evp1d_params *params, int device) {
@@ -216,7 +221,7 @@ int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6]
     nbp[k] = nb0.data() + (size_t)k * na;
   }
   evp::TilePlan plan;
-  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan);
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, g_tile_points.load());
 
   evp1d_t *h = new evp1d_handle();
   h->p = to_params(*params);
@@ -514,6 +519,16 @@ int evp1d_synchronize(evp1d_t *h) {
   return check_device_error(h);
 }
 
+int evp1d_set_tile_points(int points) {
+  if (points < 32 || points > evp::kTileOwned)
+    return fail(EVP1D_ERR_INVALID_ARG, "tile points %d outside [32, %d]", points,
+                evp::kTileOwned);
+  g_tile_points.store(points);
+  return EVP1D_OK;
+}
+
+int evp1d_get_tile_points(void) { return g_tile_points.load(); }
+
 int evp1d_debug_wait_timeout(evp1d_t *h, long long ns) {
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (ns < 1000000 || ns > 1000000000)
@@ -649,7 +664,7 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
     nbp[k] = nb0.data() + (size_t)k * na;
   }
   evp::TilePlan plan;
-  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan);
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, g_tile_points.load());
   long long hmax = 0, tmax = 0, xmax = 0;
   for (int t = 0; t < plan.ntiles; t++) {
     if (plan.halo_cnt[t] > hmax) hmax = plan.halo_cnt[t];

@@ -101,7 +101,8 @@ bool reconstruct_coords(int na, const int32_t *const nb0[6],
 
 void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
                      const int32_t *coords_i, const int32_t *coords_j,
-                     TilePlan *plan) {
+                     TilePlan *plan, int max_tile) {
+  const int tmax = max_tile < 1 ? 1 : (max_tile > kTileOwned ? kTileOwned : max_tile);
   TilePlan &P = *plan;
   P = TilePlan();
   P.na = na;
@@ -139,7 +140,7 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
     // pieces in a canonical order (by their position in the grid walk's
     // coordinates is not canonical, so by size and extent), points of a piece
     // along a Hilbert curve over its coordinates, then consecutive runs of
-    // kTileOwned points: compact, full tiles.  A run may span two pieces;
+    // tmax points: compact, full tiles.  A run may span two pieces;
     // pieces never share neighbours, so that only merges small floes.
     std::vector<int32_t> pn((size_t)nc, 0), pw((size_t)nc, 0), ph((size_t)nc, 0);
     for (int p = 0; p < na; p++) {
@@ -171,7 +172,7 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
       }
       return hkey[a] < hkey[b];
     });
-    // each tile takes the longest run (up to kTileOwned points) whose halo
+    // each tile takes the longest run (up to tmax points) whose halo
     // and velocity extras fit, found by bisection on the run length
     std::vector<int32_t> m1((size_t)navel, -1), m2((size_t)navel, -1), m3((size_t)navel, -1);
     int st = 0;
@@ -203,7 +204,7 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
       return nx <= kTileUvx;
     };
     for (int k = 0; k < na;) {
-      int len = kTileOwned < na - k ? kTileOwned : na - k;
+      int len = tmax < na - k ? tmax : na - k;
       if (!fits(k, len)) {
         int lo = 1, hi = len - 1;  // fits(k, 1) holds: a point reaches 3 + 6 + 9 others
         while (lo < hi) {
@@ -216,9 +217,9 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
       k += len;
     }
   } else {
-    for (int k = 0; k < na; k += kTileOwned) {
+    for (int k = 0; k < na; k += tmax) {
       std::vector<int32_t> g;
-      for (int p = k; p < na && p < k + kTileOwned; p++) g.push_back(p);
+      for (int p = k; p < na && p < k + tmax; p++) g.push_back(p);
       groups.push_back(std::move(g));
     }
   }
@@ -262,7 +263,7 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
         for (int r = 0; r < 3; r++) add_x(nb0[r][p]);
       for (int q : hl)
         for (int r = 0; r < 3; r++) add_x(nb0[r][q]);
-      if ((int)g.size() <= kTileOwned && nh <= kTileHalo && nx <= kTileUvx) {
+      if ((int)g.size() <= tmax && nh <= kTileHalo && nx <= kTileUvx) {
         tiles.push_back(std::move(g));
       } else {
         const size_t half = g.size() / 2;

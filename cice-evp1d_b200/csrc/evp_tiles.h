@@ -64,9 +64,10 @@ struct TilePlan {
 // Build the plan from 0-based neighbour vectors (values in [0, navel)).
 // coords_i/coords_j may be null; then (i,j) are reconstructed from the
 // neighbour graph, and if that is inconsistent the plan falls back to tiles
-// of consecutive list points.
+// of consecutive list points.  Tiles hold at most max_tile points
+// (1..kTileOwned; the kernels' shared-memory layout stays kTileOwned wide).
 void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
                      const int32_t *coords_i, const int32_t *coords_j,
-                     TilePlan *plan);
+                     TilePlan *plan, int max_tile = kTileOwned);
 
 }  // namespace evp

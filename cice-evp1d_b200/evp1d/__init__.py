@@ -105,6 +105,50 @@ def build_index(mask: np.ndarray, nghost: int = 1):
     return n, nv, ti[:n], tj[:n], tij[:nv], {k: v[:n] for k, v in nb.items()}
 
 
+def set_tile_points(points: int) -> None:
+    """Largest tile (list points, 32..256) of the plans of handles created
+    from now on (evp1d_set_tile_points); results do not depend on it."""
+    check(_lib.load().evp1d_set_tile_points(int(points)), "evp1d_set_tile_points")
+
+
+def get_tile_points() -> int:
+    return int(_lib.load().evp1d_get_tile_points())
+
+
+def tune_tile_points(prob, candidates=(256, 224, 192, 160, 128), nsub: int = 20,
+                     device: int = 0) -> tuple:
+    """The autotuner's tile-size dimension: for each candidate, build a handle
+    planned with that largest tile for `prob` (a Problem1D, or an Ensemble for
+    a batched handle), upload its fields and time `nsub` subcycles (best of
+    two).  Leaves the fastest size set for later handles and returns
+    (best, {points: microseconds per subcycle})."""
+    import time
+    batched = hasattr(prob, "combined")
+    times = {}
+    for n in candidates:
+        set_tile_points(n)
+        if batched:
+            s = EVP1D.batched(prob, device=device)
+            fs = FieldSet.from_problem(prob.combined)
+        else:
+            s = EVP1D.from_problem(prob, device=device)
+            fs = FieldSet.from_problem(prob)
+        with s:
+            s.upload(fs)
+            s.subcycles(2)
+            s.synchronize()
+            best = float("inf")
+            for _ in range(2):
+                t0 = time.perf_counter()
+                s.subcycles(nsub)
+                s.synchronize()
+                best = min(best, time.perf_counter() - t0)
+        times[int(n)] = best / nsub * 1e6
+    pick = min(times, key=times.get)
+    set_tile_points(pick)
+    return pick, times
+
+
 def plan_stats(na: int, navel: int, idx: dict) -> dict:
     """Tile plan the solver builds for these 1-based neighbour vectors (host
     only, no GPU)."""

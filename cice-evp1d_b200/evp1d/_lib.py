@@ -123,6 +123,10 @@ def load() -> C.CDLL:
     L.evp1d_adjoint_gradients.argtypes = [H, C.POINTER(Grads)]
     L.evp1d_adjoint_info.argtypes = [H, C.POINTER(C.c_longlong)]
     L.evp1d_set_adjoint_budget.argtypes = [H, C.c_longlong]
+    L.evp1d_set_tile_points.argtypes = [C.c_int]
+    L.evp1d_set_tile_points.restype = C.c_int
+    L.evp1d_get_tile_points.argtypes = []
+    L.evp1d_get_tile_points.restype = C.c_int
     for name in ("evp1d_run_checkpointed", "evp1d_record_subcycles", "evp1d_adjoint",
                  "evp1d_adjoint_seed", "evp1d_adjoint_sweep", "evp1d_adjoint_gradients",
                  "evp1d_adjoint_info", "evp1d_set_adjoint_budget"):

@@ -256,6 +256,15 @@ int evp1d_dyn_finalize(evp1d_dyn_t *handle);
 /* Number of 1D list points (nActive) and slots (navel) of a 2D handle. */
 int evp1d_dyn_sizes(evp1d_dyn_t *handle, int *na, int *navel);
 
+/* Largest tile, in list points, of the tile plans of handles created after
+ * the call (evp1d_init, evp1d_init_batched, and evp1d_plan_stats); 32..256,
+ * default 256.  Process-wide; handles that exist keep their plan.  No
+ * counterpart in the reference: a dimension for the autotuner
+ * (evp1d.tune_tile_points in the Python binding times candidate sizes on the
+ * caller's problem).  Results do not depend on it. */
+int evp1d_set_tile_points(int points);
+int evp1d_get_tile_points(void);
+
 /* ----------------------------------------------------------------------------
  * Host-only diagnostics of the tile plan the solver would build for a 1D
  * problem (same arguments as evp1d_init, 1-based neighbours; no GPU needed).

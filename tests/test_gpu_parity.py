@@ -300,6 +300,38 @@ def test_nonfinite_inputs(oracle_mod):
     assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 5), pr)
 
 
+@pytest.mark.parametrize("points", [128, 200])
+def test_smaller_tiles_bitwise(oracle_mod, points):
+    """Plans with a smaller largest tile (evp1d_set_tile_points) give the same
+    bits: the tile size is a performance choice only."""
+    pr = synth.to_1d(synth.make_grid(131, 77, seed=9, ndte=13, curvilinear=True))
+    old = evp1d.get_tile_points()
+    try:
+        evp1d.set_tile_points(points)
+        assert evp1d.plan_stats(pr.na, pr.navel, pr.idx)["max_tile"] <= points
+        fs = gpu_run(pr, 13)
+    finally:
+        evp1d.set_tile_points(old)
+    assert_same(fs, oracle_run(oracle_mod, pr, 13), pr)
+
+
+def test_tile_size_tuner():
+    """evp1d.tune_tile_points times each candidate on the caller's problem
+    (single and batched) and leaves the fastest set."""
+    old = evp1d.get_tile_points()
+    try:
+        pr = synth.make_problem("grid400x300", nx=120, ny=90, ndte=4)
+        best, times = evp1d.tune_tile_points(pr, candidates=(256, 128), nsub=4)
+        assert set(times) == {256, 128} and best in times and evp1d.get_tile_points() == best
+        assert all(t > 0 for t in times.values())
+        members = [synth.make_problem("grid400x300", nx=nx, ny=ny, seed=60 + i, ndte=4)
+                   for i, (nx, ny) in enumerate([(40, 30), (70, 55)])]
+        best, times = evp1d.tune_tile_points(synth.concat(members), candidates=(192, 256), nsub=4)
+        assert set(times) == {192, 256} and evp1d.get_tile_points() == best
+    finally:
+        evp1d.set_tile_points(old)
+
+
 def test_golden_fixture_md5():
     """The CUDA path reproduces the committed fixture's md5s and arrays."""
     import golden_io

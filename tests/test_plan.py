@@ -65,3 +65,22 @@ def test_caps_are_reached_and_kept():
     pr = helpers.random_graph_problem(5000, 300, 0)
     s = evp1d.plan_stats(pr.na, pr.navel, pr.idx)
     assert s["max_extras"] == 128 and s["max_halo"] <= 64, s
+
+
+def test_tile_points_setting():
+    """evp1d_set_tile_points bounds the tiles of later plans; values outside
+    32..256 are refused; 256 is the default."""
+    pr = synth.make_problem("grid400x300", nx=80, ny=60, ndte=3)
+    old = evp1d.get_tile_points()
+    try:
+        assert old == TILE
+        for n in (128, 200):
+            evp1d.set_tile_points(n)
+            s = evp1d.plan_stats(pr.na, pr.navel, pr.idx)
+            assert s["max_tile"] <= n and s["max_halo"] <= 64, (n, s)
+        for bad in (0, 31, 257):
+            with pytest.raises(evp1d.EVP1DError):
+                evp1d.set_tile_points(bad)
+        assert evp1d.get_tile_points() == 200
+    finally:
+        evp1d.set_tile_points(old)
