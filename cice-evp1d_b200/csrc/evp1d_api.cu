@@ -394,6 +394,7 @@ int evp1d_finalize(evp1d_t *h) {
   cudaSetDevice(h->d.device);
   drop_graphs(h);
   evp::adjoint_release(h->adj);
+  evp::exchange_release(h);
   evp::problem_destroy(&h->d);
   if (h->trace) cudaFree(h->trace);
   delete h;

@@ -7,10 +7,13 @@
 
 #include "evp_internal.h"
 
+struct evp1d_handle;
 namespace evp {
 struct AdjointState;
 // Free the adjoint buffers of a handle (NULL is a no-op).
 void adjoint_release(AdjointState *a);
+// Free the velocity-exchange lists of a handle.
+void exchange_release(evp1d_handle *h);
 // Forget the recorded forward (the inputs or parameters changed).
 void adjoint_invalidate(AdjointState *a);
 }  // namespace evp
@@ -36,5 +39,9 @@ struct evp1d_handle {
   std::vector<double> uv_tmp;  // scratch for u, v (and str) in combined order
   std::string tuned;           // last autotuner choice
   evp::AdjointState *adj = nullptr;  // checkpoints and work arrays of the adjoint
+  // velocity exchange of a split state (evp1d_exchange_*): device positions
+  // of the n_send sent points, then of the n_recv received ones
+  int32_t *xpos = nullptr;
+  int nsend = 0, nrecv = 0;
 };
 

@@ -419,6 +419,26 @@ class EVP1D:
     def stream(self) -> int:
         return self._L.evp1d_stream(self.h) or 0
 
+    # -- a state split over handles (evp1d.bands) ---------------------------
+    def exchange_setup(self, send_idx, recv_idx) -> None:
+        """Velocity-exchange lists (evp1d_exchange_setup): 1-based local list
+        points whose u, v are sent, and 1-based local positions that receive."""
+        si = np.ascontiguousarray(send_idx, dtype=np.int32)
+        ri = np.ascontiguousarray(recv_idx, dtype=np.int32)
+        check(self._L.evp1d_exchange_setup(self.h, len(si), si.ctypes.data_as(_I), len(ri),
+                                           ri.ctypes.data_as(_I)), "evp1d_exchange_setup")
+
+    def exchange_pack(self, dev_ptr: int) -> None:
+        """u, v pairs of the sent points into a device buffer (on the
+        handle's stream)."""
+        check(self._L.evp1d_exchange_pack(self.h, C.c_void_p(int(dev_ptr))),
+              "evp1d_exchange_pack")
+
+    def exchange_unpack(self, dev_ptr: int) -> None:
+        """u, v pairs from a device buffer into the received positions."""
+        check(self._L.evp1d_exchange_unpack(self.h, C.c_void_p(int(dev_ptr))),
+              "evp1d_exchange_unpack")
+
     def launch_count(self, reset: bool = False) -> int:
         return int(self._L.evp1d_launch_count(self.h, 1 if reset else 0))
 

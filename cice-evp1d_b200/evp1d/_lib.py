@@ -127,6 +127,11 @@ def load() -> C.CDLL:
     L.evp1d_set_tile_points.restype = C.c_int
     L.evp1d_get_tile_points.argtypes = []
     L.evp1d_get_tile_points.restype = C.c_int
+    L.evp1d_exchange_setup.argtypes = [H, C.c_int, _I, C.c_int, _I]
+    L.evp1d_exchange_pack.argtypes = [H, C.c_void_p]
+    L.evp1d_exchange_unpack.argtypes = [H, C.c_void_p]
+    for name in ("evp1d_exchange_setup", "evp1d_exchange_pack", "evp1d_exchange_unpack"):
+        getattr(L, name).restype = C.c_int
     for name in ("evp1d_run_checkpointed", "evp1d_record_subcycles", "evp1d_adjoint",
                  "evp1d_adjoint_seed", "evp1d_adjoint_sweep", "evp1d_adjoint_gradients",
                  "evp1d_adjoint_info", "evp1d_set_adjoint_budget"):

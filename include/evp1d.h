@@ -266,6 +266,32 @@ int evp1d_set_tile_points(int points);
 int evp1d_get_tile_points(void);
 
 /* ----------------------------------------------------------------------------
+ * Velocity exchange of one state split over several handles (one per GPU).
+ * No counterpart in the reference, which gathers the whole domain onto the
+ * master task before the 1D solver runs (gather_global_ext,
+ * integration/ice_dyn_evp1d.F90:637-716).
+ *
+ * Each handle holds a band of the global list plus ghost points: the stepu
+ * neighbours of its band (solved for stress here, skipU set) and the other
+ * points whose velocities its stress reads (halo slots).  After every
+ * subcycle, the caller gathers the band's boundary velocities, moves them to
+ * the handles that hold them as ghosts, and scatters them there.
+ *   evp1d_exchange_setup:  send_idx are the 1-based local list points
+ *                          (1..na) whose u, v the handle sends; recv_idx are
+ *                          the 1-based local positions (1..navel, no repeats)
+ *                          that receive u, v.
+ *   evp1d_exchange_pack:   device buffer[2k], [2k+1] = u, v of send_idx[k] in
+ *                          the current state (2 x n_send doubles).
+ *   evp1d_exchange_unpack: u, v of recv_idx[k] in the current state =
+ *                          device buffer[2k], [2k+1] (2 x n_recv doubles).
+ * Both run on the handle's stream (evp1d_stream) and do not wait for it.
+ * Single-state handles only (not evp1d_init_batched). */
+int evp1d_exchange_setup(evp1d_t *handle, int n_send, const int32_t *send_idx, int n_recv,
+                         const int32_t *recv_idx);
+int evp1d_exchange_pack(evp1d_t *handle, double *dev_buffer);
+int evp1d_exchange_unpack(evp1d_t *handle, const double *dev_buffer);
+
+/* ----------------------------------------------------------------------------
  * Host-only diagnostics of the tile plan the solver would build for a 1D
  * problem (same arguments as evp1d_init, 1-based neighbours; no GPU needed).
  * stats[0] tiles, [1] device slots (list points + alignment padding),
