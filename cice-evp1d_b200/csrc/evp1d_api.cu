@@ -18,6 +18,8 @@ using evp::Params;
 
 namespace {
 thread_local std::string g_err;
+// allocations left until the injected failure (0: none armed)
+std::atomic<int> g_fail_alloc{0};
 }  // namespace
 
 namespace evp {
@@ -29,6 +31,17 @@ int error(int code, const char *fmt, ...) {
   va_end(ap);
   g_err = buf;
   return code;
+}
+
+cudaError_t device_alloc(void **p, size_t bytes) {
+  int n = g_fail_alloc.load();
+  while (n > 0 && !g_fail_alloc.compare_exchange_weak(n, n - 1)) {
+  }
+  if (n == 1) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
 }
 }  // namespace evp
 
@@ -229,7 +242,7 @@ int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6]
     if (!strcmp(e, "fused")) h->path = kPathFused;
   }
   if (getenv("EVP1D_TRACE")) {
-    if (cudaMalloc(&h->trace, sizeof(long long) * 8 * evp::kTraceTiles) != cudaSuccess)
+    if (evp::device_alloc(&h->trace, sizeof(long long) * 8 * evp::kTraceTiles) != cudaSuccess)
       h->trace = nullptr;
     else
       cudaMemset(h->trace, 0, sizeof(long long) * 8 * evp::kTraceTiles);
@@ -540,6 +553,12 @@ int evp1d_debug_wait_timeout(evp1d_t *h, long long ns) {
   return EVP1D_OK;
 }
 
+int evp1d_debug_fail_alloc(int n) {
+  if (n < 0) return fail(EVP1D_ERR_INVALID_ARG, "n = %d < 0", n);
+  g_fail_alloc.store(n);
+  return EVP1D_OK;
+}
+
 int evp1d_debug_trace(evp1d_t *h, long long *out, int n) {
   if (!h || !out || n < 0) return fail(EVP1D_ERR_INVALID_ARG, "bad arguments");
   if (!h->trace) return fail(EVP1D_ERR_STATE, "tracing is off (set EVP1D_TRACE)");
@@ -572,7 +591,7 @@ int evp1d_autotune(evp1d_t *h, int nsub, char *chosen, int len) {
   size_t total = 0;
   for (auto &a : arrs) total += a.second;
   double *backup = nullptr;
-  CUDA_TRY(cudaMalloc(&backup, total * sizeof(double)));
+  CUDA_TRY(evp::device_alloc(&backup, total * sizeof(double)));
   auto copy_all = [&](bool save) {
     size_t o = 0;
     for (auto &a : arrs) {

@@ -374,7 +374,7 @@ int ensure_static(evp1d_t *h) {
   for (int t = 0; t < kNumTr; t++) ints += pad_ints(off[t].size()) + pad_ints(idx[t].size() + 1);
   const size_t ndbl = SD * (4 + 8 + 12 + kNumGrad + 24);
   A.arena_bytes = ints * sizeof(int32_t) + ndbl * sizeof(double);
-  ADJ_TRY(cudaMalloc(&A.arena, A.arena_bytes));
+  ADJ_TRY(device_alloc(&A.arena, A.arena_bytes));
   double *pd = (double *)A.arena;
   auto take = [&]() {
     double *r = pd;
@@ -499,7 +499,7 @@ int ensure_store(AdjointState &A, size_t bytes) {
   if (A.store) cudaFree(A.store);
   A.store = nullptr;
   A.store_bytes = 0;
-  ADJ_TRY(cudaMalloc(&A.store, bytes));
+  ADJ_TRY(device_alloc(&A.store, bytes));
   A.store_bytes = bytes;
   return EVP1D_OK;
 }

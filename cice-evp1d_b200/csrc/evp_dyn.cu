@@ -160,9 +160,9 @@ int evp1d_dyn_init(evp1d_dyn_t **handle, int nx, int ny, int nghost,
   }
   if (na > 0) {
     const size_t cells = (size_t)nx * ny;
-    cudaError_t e = cudaMalloc(&d->cell, sizeof(int32_t) * (size_t)na);
-    if (e == cudaSuccess) e = cudaMalloc(&d->f2d, sizeof(double) * kF2d * cells);
-    if (e == cudaSuccess) e = cudaMalloc(&d->mask2d, sizeof(int32_t) * 2 * cells);
+    cudaError_t e = evp::device_alloc(&d->cell, sizeof(int32_t) * (size_t)na);
+    if (e == cudaSuccess) e = evp::device_alloc(&d->f2d, sizeof(double) * kF2d * cells);
+    if (e == cudaSuccess) e = evp::device_alloc(&d->mask2d, sizeof(int32_t) * 2 * cells);
     if (e == cudaSuccess)
       e = cudaMemcpy(d->cell, cell.data(), sizeof(int32_t) * (size_t)na, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {

@@ -98,7 +98,7 @@ int evp1d_exchange_setup(evp1d_t *h, int n_send, const int32_t *send_idx, int n_
   const int n = n_send + n_recv;
   if (n == 0) return EVP1D_OK;
   cudaStream_t st = h->d.stream;
-  cudaError_t e = cudaMalloc(&h->xpos, sizeof(int32_t) * (size_t)n);
+  cudaError_t e = evp::device_alloc(&h->xpos, sizeof(int32_t) * (size_t)n);
   if (e != cudaSuccess) {
     h->xpos = nullptr;
     return cuda_fail(e, "cudaMalloc");

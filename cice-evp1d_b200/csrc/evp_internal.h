@@ -26,6 +26,15 @@ struct NvtxRange {
   NvtxRange &operator=(const NvtxRange &) = delete;
 };
 
+// Every device allocation of the library: cudaMalloc, unless the failure
+// injection of evp1d_debug_fail_alloc picks this allocation, which then
+// fails with cudaErrorMemoryAllocation and allocates nothing.
+cudaError_t device_alloc(void **p, size_t bytes);
+template <class T>
+cudaError_t device_alloc(T **p, size_t bytes) {
+  return device_alloc(reinterpret_cast<void **>(p), bytes);
+}
+
 // Per-call input fields in the order they are staged and scattered.
 enum DynField {
   kStrength, kCw, kAiu, kUocn, kVocn, kWaterx, kWatery, kForcex, kForcey,

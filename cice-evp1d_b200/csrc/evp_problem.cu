@@ -106,7 +106,7 @@ int problem_create(DeviceProblem *d, int device, const TilePlan &plan,
     return error(EVP1D_ERR_CUDA, "cannot enable %d bytes of shared memory", 0);
   Carve sizing;
   layout(d, sizing, plan.halo_idx.size(), plan.uvx_idx.size());
-  CUDA_TRY(cudaMalloc(&d->arena, sizing.off));
+  CUDA_TRY(device_alloc(&d->arena, sizing.off));
   d->arena_bytes = sizing.off;
   Carve c;
   c.base = (char *)d->arena;

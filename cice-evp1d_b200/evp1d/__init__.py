@@ -149,6 +149,12 @@ def tune_tile_points(prob, candidates=(256, 224, 192, 160, 128), nsub: int = 20,
     return pick, times
 
 
+def debug_fail_alloc(n: int) -> None:
+    """Host-side fault injection (evp1d_debug_fail_alloc): the n-th device
+    allocation of the library from now on fails as out of memory; 0 disarms."""
+    check(_lib.load().evp1d_debug_fail_alloc(int(n)), "evp1d_debug_fail_alloc")
+
+
 def plan_stats(na: int, navel: int, idx: dict) -> dict:
     """Tile plan the solver builds for these 1-based neighbour vectors (host
     only, no GPU)."""

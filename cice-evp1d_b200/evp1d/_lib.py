@@ -127,6 +127,8 @@ def load() -> C.CDLL:
     L.evp1d_set_tile_points.restype = C.c_int
     L.evp1d_get_tile_points.argtypes = []
     L.evp1d_get_tile_points.restype = C.c_int
+    L.evp1d_debug_fail_alloc.argtypes = [C.c_int]
+    L.evp1d_debug_fail_alloc.restype = C.c_int
     L.evp1d_exchange_setup.argtypes = [H, C.c_int, _I, C.c_int, _I]
     L.evp1d_exchange_pack.argtypes = [H, C.c_void_p]
     L.evp1d_exchange_unpack.argtypes = [H, C.c_void_p]

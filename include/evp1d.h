@@ -170,6 +170,14 @@ int evp1d_synchronize(evp1d_t *handle);
  * and clears it; the handle stays usable. */
 int evp1d_debug_wait_timeout(evp1d_t *handle, long long ns);
 
+/* Debug: host-side injection of an out-of-memory failure.  The n-th device
+ * allocation of the library after this call (1 = the next one) fails as if
+ * the device were full: it allocates nothing, and the call that made it
+ * returns EVP1D_ERR_NOMEM after freeing what it had allocated.  0 disarms.
+ * Process-wide.  The reference stops the program on a failed allocation
+ * instead (integration/ice_dyn_evp1d.F90:394-460). */
+int evp1d_debug_fail_alloc(int n);
+
 /* Debug: timing trace of the TMA kernel's block 0 in the last launch
  * (recorded only when EVP1D_TRACE is set at evp1d_init).  Up to 256 tiles x 8
  * %globaltimer stamps (ns): [0] the producer warps issued all of the tile's
