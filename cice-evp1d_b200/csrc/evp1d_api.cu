@@ -235,6 +235,13 @@ int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6]
   }
   evp::TilePlan plan;
   evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, g_tile_points.load());
+  if (getenv("EVP1D_CHECK_PLAN")) {
+    std::string first;
+    const long long bad = evp::verify_tile_plan(plan, nbp, g_tile_points.load(), &first);
+    if (bad)
+      return fail(EVP1D_ERR_INDEX, "tile plan: %lld violations, the first: %s", bad,
+                  first.c_str());
+  }
 
   evp1d_t *h = new evp1d_handle();
   h->p = to_params(*params);
@@ -665,16 +672,15 @@ const char *evp1d_kernel_path(evp1d_t *h) {
   return h->path == kPathTma ? "fused-tile-tma" : "fused-tile";
 }
 
-int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
-                     const int32_t *se, const int32_t *nw, const int32_t *sw,
-                     const int32_t *sse, long long stats[8]) {
-  if (!stats || na < 0 || navel < na)
-    return fail(EVP1D_ERR_INVALID_ARG, "bad arguments");
-  const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
+namespace {
+// The host half of evp1d_init for the plan diagnostics: checked 1-based
+// neighbour vectors -> 0-based copies (nb0, nbp) -> the tile plan.
+int plan_from_vectors(int na, int navel, const int32_t *const idx[6], std::vector<int32_t> &nb0,
+                      const int32_t *nbp[6], evp::TilePlan *plan) {
+  if (na < 0 || navel < na) return fail(EVP1D_ERR_INVALID_ARG, "bad arguments");
   if (na > 0 && !nonnull_all((const void *const *)idx, 6))
     return fail(EVP1D_ERR_INVALID_ARG, "a neighbour vector is NULL");
-  std::vector<int32_t> nb0((size_t)na * 6);
-  const int32_t *nbp[6];
+  nb0.assign((size_t)na * 6, 0);
   for (int k = 0; k < 6; k++) {
     for (int w = 0; w < na; w++) {
       const int32_t v = idx[k][w];
@@ -683,8 +689,36 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
     }
     nbp[k] = nb0.data() + (size_t)k * na;
   }
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, plan, g_tile_points.load());
+  return EVP1D_OK;
+}
+}  // namespace
+
+int evp1d_plan_check(int na, int navel, const int32_t *ee, const int32_t *ne,
+                     const int32_t *se, const int32_t *nw, const int32_t *sw,
+                     const int32_t *sse, long long *violations) {
+  const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
+  std::vector<int32_t> nb0;
+  const int32_t *nbp[6] = {};
   evp::TilePlan plan;
-  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, g_tile_points.load());
+  CHECK(plan_from_vectors(na, navel, idx, nb0, nbp, &plan));
+  std::string first;
+  const long long bad = evp::verify_tile_plan(plan, nbp, g_tile_points.load(), &first);
+  if (violations) *violations = bad;
+  if (bad)
+    return fail(EVP1D_ERR_INDEX, "tile plan: %lld violations, the first: %s", bad, first.c_str());
+  return EVP1D_OK;
+}
+
+int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
+                     const int32_t *se, const int32_t *nw, const int32_t *sw,
+                     const int32_t *sse, long long stats[8]) {
+  if (!stats) return fail(EVP1D_ERR_INVALID_ARG, "bad arguments");
+  const int32_t *idx[6] = {ee, ne, se, nw, sw, sse};
+  std::vector<int32_t> nb0;
+  const int32_t *nbp[6] = {};
+  evp::TilePlan plan;
+  CHECK(plan_from_vectors(na, navel, idx, nb0, nbp, &plan));
   long long hmax = 0, tmax = 0, xmax = 0;
   for (int t = 0; t < plan.ntiles; t++) {
     if (plan.halo_cnt[t] > hmax) hmax = plan.halo_cnt[t];

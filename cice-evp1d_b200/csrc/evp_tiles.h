@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace evp {
@@ -69,5 +70,13 @@ struct TilePlan {
 void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
                      const int32_t *coords_i, const int32_t *coords_j,
                      TilePlan *plan, int max_tile = kTileOwned);
+
+// Decode every index of `plan` that the kernels gather through (slot maps,
+// tile ranges, neighbour slots, forward halos, velocity extras, the packed
+// local indices) and compare it with what the 0-based neighbour vectors say
+// it must be.  Returns the number of violations; *first (if not null) then
+// describes the first one.  Host only (evp_plan_check.cpp).
+long long verify_tile_plan(const TilePlan &plan, const int32_t *const nb0[6], int max_tile,
+                           std::string *first);
 
 }  // namespace evp

@@ -155,6 +155,17 @@ def debug_fail_alloc(n: int) -> None:
     check(_lib.load().evp1d_debug_fail_alloc(int(n)), "evp1d_debug_fail_alloc")
 
 
+def plan_check(na: int, navel: int, idx: dict) -> None:
+    """Build the tile plan for these 1-based neighbour vectors and verify
+    every index the kernels gather through (evp1d_plan_check; host only).
+    Raises EVP1DError (EVP1D_ERR_INDEX) naming the first violation."""
+    L = _lib.load()
+    n = C.c_longlong(0)
+    arrs = [_as_i32(idx[k], na, k) for k in ("ee", "ne", "se", "nw", "sw", "sse")]
+    check(L.evp1d_plan_check(int(na), int(navel), *[a.ctypes.data_as(_I) for a in arrs],
+                             C.byref(n)), "evp1d_plan_check")
+
+
 def plan_stats(na: int, navel: int, idx: dict) -> dict:
     """Tile plan the solver builds for these 1-based neighbour vectors (host
     only, no GPU)."""

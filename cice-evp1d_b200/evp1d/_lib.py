@@ -115,6 +115,7 @@ def load() -> C.CDLL:
                                      C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)] + [_I] * 9)
     L.evp1d_plan_stats.argtypes = [C.c_int, C.c_int] + [_I] * 6 + [C.POINTER(C.c_longlong)]
+    L.evp1d_plan_check.argtypes = [C.c_int, C.c_int] + [_I] * 6 + [C.POINTER(C.c_longlong)]
     L.evp1d_run_checkpointed.argtypes = [H, C.c_int, C.POINTER(Fields), C.c_int]
     L.evp1d_record_subcycles.argtypes = [H, C.c_int, C.c_int]
     L.evp1d_adjoint.argtypes = [H, _D, _D, C.POINTER(_D), C.POINTER(Grads)]
@@ -146,7 +147,7 @@ def load() -> C.CDLL:
                                            + [C.POINTER(Params), C.c_int,
                                               C.POINTER(Fields), C.c_void_p])
     L.evp1d_run_device_noalloc.restype = C.c_int
-    for name in ("evp1d_plan_stats", "evp1d_init", "evp1d_finalize", "evp1d_set_params",
+    for name in ("evp1d_plan_stats", "evp1d_plan_check", "evp1d_init", "evp1d_finalize", "evp1d_set_params",
                  "evp1d_run", "evp1d_upload", "evp1d_subcycles",
                  "evp1d_download", "evp1d_stress_only", "evp1d_stepu_only",
                  "evp1d_synchronize", "evp1d_build_index"):

@@ -312,6 +312,16 @@ int evp1d_exchange_unpack(evp1d_t *handle, const double *dev_buffer);
 int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
                      const int32_t *se, const int32_t *nw, const int32_t *sw,
                      const int32_t *sse, long long stats[8]);
+/* Builds the same plan and decodes every index the kernels gather through
+ * (slot maps, tile ranges, neighbour slots, forward halos, extra velocity
+ * points, the packed local indices), comparing each with what the neighbour
+ * vectors say it must be.  EVP1D_OK, or EVP1D_ERR_INDEX naming the first
+ * violation; *violations (may be NULL) gets their number.  Host only.  With
+ * the environment variable EVP1D_CHECK_PLAN set, evp1d_init and
+ * evp1d_init_batched run the same check and refuse a plan that fails it. */
+int evp1d_plan_check(int na, int navel, const int32_t *ee, const int32_t *ne,
+                     const int32_t *se, const int32_t *nw, const int32_t *sw,
+                     const int32_t *sse, long long *violations);
 
 /* ----------------------------------------------------------------------------
  * Adjoint (reverse-mode gradients) of the subcycle loop.  No counterpart in

@@ -11,6 +11,10 @@ for p in (PKG, ORACLE, ROOT):
     if p not in sys.path:
         sys.path.insert(0, p)
 
+# every handle the tests create first verifies its tile plan on the host
+# (evp1d_plan_check); a wrong derived index fails evp1d_init
+os.environ.setdefault("EVP1D_CHECK_PLAN", "1")
+
 
 def pytest_configure(config):
     config.addinivalue_line(

@@ -84,3 +84,74 @@ def test_tile_points_setting():
         assert evp1d.get_tile_points() == 200
     finally:
         evp1d.set_tile_points(old)
+
+
+# ---- the plan verifier (evp1d_plan_check) ------------------------------------
+
+def _check(pr):
+    evp1d.plan_check(pr.na, pr.navel, pr.idx)
+
+
+@pytest.mark.parametrize("points", [256, 200, 128, 37])
+def test_plan_check_passes_on_grids(points):
+    old = evp1d.get_tile_points()
+    try:
+        evp1d.set_tile_points(points)
+        _check(synth.to_1d(synth.make_grid(131, 77, seed=9, ndte=2, curvilinear=True)))
+        _check(helpers.shuffle_problem(synth.make_problem("grid400x300", nx=90, ny=70, ndte=2), 3))
+    finally:
+        evp1d.set_tile_points(old)
+
+
+def test_plan_check_passes_on_the_reference_shaped_problems():
+    _check(synth.make_problem("grid400x300"))
+    _check(helpers.standalone_problem())
+    for na, nhalo, seed in ((5000, 300, 0), (777, 5, 1), (1, 1, 2)):
+        _check(helpers.random_graph_problem(na, nhalo, seed))
+    evp1d.plan_check(0, 0, {k: np.zeros(0, np.int32) for k in ("ee", "ne", "se", "nw", "sw", "sse")})
+
+
+def test_plan_check_passes_on_band_problems():
+    """The local problems of a state split into bands (ring points, ghost
+    halo slots, partial rows)."""
+    from evp1d import bands
+    pr = synth.to_1d(synth.make_grid(131, 77, seed=9, ndte=2, curvilinear=True))
+    for nb in (2, 5, pr.na // 40):
+        for b in bands.split(pr, nb):
+            _check(b.local)
+
+
+@pytest.fixture(scope="module")
+def plan_shim(tmp_path_factory):
+    import ctypes as C
+    import os
+    import subprocess
+    from conftest import PKG, ROOT
+    out = str(tmp_path_factory.mktemp("plan") / "plan_check_shim.so")
+    csrc = os.path.join(PKG, "csrc")
+    subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-I", csrc,
+                    os.path.join(csrc, "evp_tiles.cpp"), os.path.join(csrc, "evp_plan_check.cpp"),
+                    os.path.join(ROOT, "tests", "native", "plan_check_shim.cpp"), "-o", out],
+                   check=True)
+    L = C.CDLL(out)
+    L.shim_kinds.restype = C.c_int
+    L.shim_plan_check.restype = C.c_longlong
+    L.shim_plan_check.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p), C.c_int, C.c_int,
+                                  C.c_char_p, C.c_int]
+    return L
+
+
+@pytest.mark.parametrize("max_tile", [256, 128])
+def test_plan_check_catches_planted_mistakes(plan_shim, max_tile):
+    """One wrong index of each kind, planted in a plan on the host, is caught
+    (the verifier is not vacuous)."""
+    import ctypes as C
+    pr = synth.to_1d(synth.make_grid(90, 60, seed=12, ndte=2, curvilinear=True))
+    arrs = [np.ascontiguousarray(pr.idx[k], dtype=np.int32) for k in ("ee", "ne", "se", "nw", "sw", "sse")]
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    msg = C.create_string_buffer(256)
+    assert plan_shim.shim_plan_check(pr.na, pr.navel, ptrs, max_tile, 0, msg, 256) == 0
+    for kind in range(1, plan_shim.shim_kinds() + 1):
+        n = plan_shim.shim_plan_check(pr.na, pr.navel, ptrs, max_tile, kind, msg, 256)
+        assert n > 0, (kind, n)
+        assert msg.value, kind
