@@ -69,6 +69,7 @@ namespace evp {
 void exchange_release(evp1d_t *h) {
   if (h->xpos) cudaFree(h->xpos);
   h->xpos = nullptr;
+  h->xbuf = nullptr;
   h->nsend = h->nrecv = 0;
 }
 }  // namespace evp
@@ -98,11 +99,15 @@ int evp1d_exchange_setup(evp1d_t *h, int n_send, const int32_t *send_idx, int n_
   const int n = n_send + n_recv;
   if (n == 0) return EVP1D_OK;
   cudaStream_t st = h->d.stream;
-  cudaError_t e = evp::device_alloc(&h->xpos, sizeof(int32_t) * (size_t)n);
+  // one allocation: the positions, then (256-byte aligned) the send and the
+  // receive buffer of u, v pairs
+  const size_t pos_bytes = (sizeof(int32_t) * (size_t)n + 255) & ~(size_t)255;
+  cudaError_t e = evp::device_alloc(&h->xpos, pos_bytes + sizeof(double) * 2 * (size_t)n);
   if (e != cudaSuccess) {
     h->xpos = nullptr;
     return cuda_fail(e, "cudaMalloc");
   }
+  h->xbuf = reinterpret_cast<double *>(reinterpret_cast<char *>(h->xpos) + pos_bytes);
   std::vector<int32_t> all((size_t)n);
   for (int k = 0; k < n_send; k++) all[k] = send_idx[k];
   for (int k = 0; k < n_recv; k++) all[n_send + k] = recv_idx[k];
@@ -129,7 +134,7 @@ int evp1d_exchange_pack(evp1d_t *h, double *buf) {
   if (rc != EVP1D_OK) return rc;
   if (!h->uploaded) return evp::error(EVP1D_ERR_STATE, "evp1d_upload has not been called");
   if (h->nsend == 0) return EVP1D_OK;
-  if (!buf) return evp::error(EVP1D_ERR_INVALID_ARG, "NULL buffer");
+  if (!buf) buf = h->xbuf;
   const int c = h->d.cur;
   k_exchange_pack<<<blocks_for(h->nsend), kBlock, 0, h->d.stream>>>(h->nsend, h->xpos,
                                                                    h->d.u[c], h->d.v[c], buf);
@@ -144,11 +149,20 @@ int evp1d_exchange_unpack(evp1d_t *h, const double *buf) {
   if (rc != EVP1D_OK) return rc;
   if (!h->uploaded) return evp::error(EVP1D_ERR_STATE, "evp1d_upload has not been called");
   if (h->nrecv == 0) return EVP1D_OK;
-  if (!buf) return evp::error(EVP1D_ERR_INVALID_ARG, "NULL buffer");
+  if (!buf) buf = h->xbuf + 2 * (size_t)h->nsend;
   const int c = h->d.cur;
   k_exchange_unpack<<<blocks_for(h->nrecv), kBlock, 0, h->d.stream>>>(
       h->nrecv, h->xpos + h->nsend, buf, h->d.u[c], h->d.v[c]);
   h->launches++;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? EVP1D_OK : cuda_fail(e, "k_exchange_unpack");
+}
+
+int evp1d_exchange_buffers(evp1d_t *h, double **send, double **recv) {
+  int rc = usable(h);
+  if (rc != EVP1D_OK) return rc;
+  if (!send || !recv) return evp::error(EVP1D_ERR_INVALID_ARG, "NULL argument");
+  *send = h->nsend > 0 ? h->xbuf : nullptr;
+  *recv = h->nrecv > 0 ? h->xbuf + 2 * (size_t)h->nsend : nullptr;
+  return EVP1D_OK;
 }

@@ -42,6 +42,7 @@ struct evp1d_handle {
   // velocity exchange of a split state (evp1d_exchange_*): device positions
   // of the n_send sent points, then of the n_recv received ones
   int32_t *xpos = nullptr;
+  double *xbuf = nullptr;  // in the same allocation: send, then receive buffer
   int nsend = 0, nrecv = 0;
 };
 

@@ -445,16 +445,25 @@ class EVP1D:
         check(self._L.evp1d_exchange_setup(self.h, len(si), si.ctypes.data_as(_I), len(ri),
                                            ri.ctypes.data_as(_I)), "evp1d_exchange_setup")
 
-    def exchange_pack(self, dev_ptr: int) -> None:
-        """u, v pairs of the sent points into a device buffer (on the
-        handle's stream)."""
-        check(self._L.evp1d_exchange_pack(self.h, C.c_void_p(int(dev_ptr))),
+    def exchange_pack(self, dev_ptr: int = 0) -> None:
+        """u, v pairs of the sent points into a device buffer (0: the
+        handle's own send buffer), on the handle's stream."""
+        check(self._L.evp1d_exchange_pack(self.h, C.c_void_p(int(dev_ptr) or None)),
               "evp1d_exchange_pack")
 
-    def exchange_unpack(self, dev_ptr: int) -> None:
-        """u, v pairs from a device buffer into the received positions."""
-        check(self._L.evp1d_exchange_unpack(self.h, C.c_void_p(int(dev_ptr))),
+    def exchange_unpack(self, dev_ptr: int = 0) -> None:
+        """u, v pairs from a device buffer (0: the handle's own receive
+        buffer) into the received positions."""
+        check(self._L.evp1d_exchange_unpack(self.h, C.c_void_p(int(dev_ptr) or None)),
               "evp1d_exchange_unpack")
+
+    def exchange_buffers(self) -> tuple:
+        """Device addresses (send, receive) of the handle's own exchange
+        buffers; 0 where a list is empty."""
+        snd, rcv = C.c_void_p(), C.c_void_p()
+        check(self._L.evp1d_exchange_buffers(self.h, C.byref(snd), C.byref(rcv)),
+              "evp1d_exchange_buffers")
+        return snd.value or 0, rcv.value or 0
 
     def launch_count(self, reset: bool = False) -> int:
         return int(self._L.evp1d_launch_count(self.h, 1 if reset else 0))

@@ -133,7 +133,9 @@ def load() -> C.CDLL:
     L.evp1d_exchange_setup.argtypes = [H, C.c_int, _I, C.c_int, _I]
     L.evp1d_exchange_pack.argtypes = [H, C.c_void_p]
     L.evp1d_exchange_unpack.argtypes = [H, C.c_void_p]
-    for name in ("evp1d_exchange_setup", "evp1d_exchange_pack", "evp1d_exchange_unpack"):
+    L.evp1d_exchange_buffers.argtypes = [H, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    for name in ("evp1d_exchange_setup", "evp1d_exchange_pack", "evp1d_exchange_unpack",
+                 "evp1d_exchange_buffers"):
         getattr(L, name).restype = C.c_int
     for name in ("evp1d_run_checkpointed", "evp1d_record_subcycles", "evp1d_adjoint",
                  "evp1d_adjoint_seed", "evp1d_adjoint_sweep", "evp1d_adjoint_gradients",

@@ -288,16 +288,25 @@ int evp1d_get_tile_points(void);
  *                          (1..na) whose u, v the handle sends; recv_idx are
  *                          the 1-based local positions (1..navel, no repeats)
  *                          that receive u, v.
+ *                          It also allocates a send and a receive buffer
+ *                          on the device (evp1d_exchange_buffers).
  *   evp1d_exchange_pack:   device buffer[2k], [2k+1] = u, v of send_idx[k] in
- *                          the current state (2 x n_send doubles).
+ *                          the current state (2 x n_send doubles); a NULL
+ *                          buffer means the handle's send buffer.
  *   evp1d_exchange_unpack: u, v of recv_idx[k] in the current state =
- *                          device buffer[2k], [2k+1] (2 x n_recv doubles).
- * Both run on the handle's stream (evp1d_stream) and do not wait for it.
- * Single-state handles only (not evp1d_init_batched). */
+ *                          device buffer[2k], [2k+1] (2 x n_recv doubles); a
+ *                          NULL buffer means the handle's receive buffer.
+ *   evp1d_exchange_buffers: device addresses of the handle's send and
+ *                          receive buffers (NULL when empty), valid until the
+ *                          next setup or finalize: what CUDA-aware MPI or
+ *                          NCCL sends from and receives into.
+ * Pack and unpack run on the handle's stream (evp1d_stream) and do not wait
+ * for it.  Single-state handles only (not evp1d_init_batched). */
 int evp1d_exchange_setup(evp1d_t *handle, int n_send, const int32_t *send_idx, int n_recv,
                          const int32_t *recv_idx);
 int evp1d_exchange_pack(evp1d_t *handle, double *dev_buffer);
 int evp1d_exchange_unpack(evp1d_t *handle, const double *dev_buffer);
+int evp1d_exchange_buffers(evp1d_t *handle, double **send, double **recv);
 
 /* ----------------------------------------------------------------------------
  * Host-only diagnostics of the tile plan the solver would build for a 1D

@@ -34,7 +34,23 @@ def _outs(fs):
                 strinty=fs.strinty, Cb=fs.Cb)
 
 
-def solve_bands_one_gpu(pr, nbands, ndte):
+class _DeviceArray:
+    """A library-owned device buffer seen by torch without a copy."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 3}
+
+
+def _wrap(ptr, n, dev):
+    if n == 0:
+        return torch.zeros(0, dtype=torch.float64, device=dev)
+    return torch.as_tensor(_DeviceArray(ptr, n), device=dev)
+
+
+def solve_bands_one_gpu(pr, nbands, ndte, own_buffers=False):
+    """own_buffers: pack into and unpack from the handles' own exchange
+    buffers (evp1d_exchange_buffers) instead of caller buffers."""
     bs = B.split(pr, nbands)
     dev = torch.device("cuda", 0)
     hs, fss, sbuf, rbuf = [], [], [], []
@@ -46,13 +62,20 @@ def solve_bands_one_gpu(pr, nbands, ndte):
             s.upload(fs)
             hs.append(s)
             fss.append(fs)
-            sbuf.append(torch.zeros(2 * len(b.send_idx()), dtype=torch.float64, device=dev))
-            rbuf.append(torch.zeros(2 * len(b.recv_idx()), dtype=torch.float64, device=dev))
+            ns, nr = 2 * len(b.send_idx()), 2 * len(b.recv_idx())
+            if own_buffers:
+                ps, pr_ = s.exchange_buffers()
+                assert (ps != 0) == (ns > 0) and (pr_ != 0) == (nr > 0)
+                sbuf.append(_wrap(ps, ns, dev))
+                rbuf.append(_wrap(pr_, nr, dev))
+            else:
+                sbuf.append(torch.zeros(ns, dtype=torch.float64, device=dev))
+                rbuf.append(torch.zeros(nr, dtype=torch.float64, device=dev))
         for _ in range(ndte):
             for s in hs:
                 s.subcycles(1)
             for s, buf in zip(hs, sbuf):
-                s.exchange_pack(buf.data_ptr())
+                s.exchange_pack(0 if own_buffers else buf.data_ptr())
             for s in hs:
                 s.synchronize()
             torch.cuda.synchronize()
@@ -64,7 +87,7 @@ def solve_bands_one_gpu(pr, nbands, ndte):
                     buf[2 * o: 2 * (o + n)].copy_(sbuf[q][2 * so: 2 * (so + n)])
             torch.cuda.synchronize()
             for s, buf in zip(hs, rbuf):
-                s.exchange_unpack(buf.data_ptr())
+                s.exchange_unpack(0 if own_buffers else buf.data_ptr())
         for s, fs in zip(hs, fss):
             s.download(fs)
     finally:
@@ -73,10 +96,10 @@ def solve_bands_one_gpu(pr, nbands, ndte):
     return B.assemble(pr, bs, [_outs(fs) for fs in fss])
 
 
-@pytest.mark.parametrize("nbands", [2, 3, 6])
-def test_bands_on_one_gpu_bitwise(oracle_mod, nbands):
+@pytest.mark.parametrize("nbands,own", [(2, False), (3, False), (6, False), (3, True)])
+def test_bands_on_one_gpu_bitwise(oracle_mod, nbands, own):
     pr = synth.to_1d(synth.make_grid(131, 77, seed=9, ndte=13, curvilinear=True))
-    _same(solve_bands_one_gpu(pr, nbands, 13), oracle_run(oracle_mod, pr, 13), pr)
+    _same(solve_bands_one_gpu(pr, nbands, 13, own_buffers=own), oracle_run(oracle_mod, pr, 13), pr)
 
 
 def test_band_solver_world_size_one(oracle_mod):
