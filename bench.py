@@ -57,6 +57,9 @@ def parse():
                     help="target CPU time of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--split", action="store_true",
+                    help="one state of --config split into one band per rank, with a "
+                         "velocity exchange (NCCL) every subcycle: strong scaling")
     return ap.parse_args()
 
 
@@ -575,6 +578,122 @@ def run_adjoint_batched(args, rank, world, local):
         }), flush=True)
 
 
+def run_split(args, rank, world, local):
+    """--split: ONE state of the configuration split into `world` bands of
+    the 1D list, one per rank (evp1d.bands).  Each rank solves its band and
+    the band's forward ring; after every subcycle the ghost velocities move
+    between the bands by NCCL send/recv (bands.run_band).  Strong scaling of
+    the fixed state, timed on the device as the slowest rank.  The results
+    are bit-identical to the single-domain run."""
+    import torch
+    import evp1d
+    from evp1d import synth, bands, roofline as alg_bytes
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    over = {"ndte": args.ndte} if args.ndte else {}
+    pr = synth.make_problem(args.config, **over)
+    ndte = pr.ndte
+    band = bands.split(pr, world)[rank]
+    bsol = bands.BandSolver(band, ndte=ndte, device=local)
+    s = bsol.s
+    stream = torch.cuda.ExternalStream(s.stream, device=local)
+
+    def sweep(n):
+        with torch.cuda.stream(stream):
+            bands.run_band(band, n, lambda: s.subcycles(1),
+                           lambda b: s.exchange_pack(b.data_ptr()),
+                           lambda b: s.exchange_unpack(b.data_ptr()),
+                           bsol.send_buf, bsol.recv_buf)
+
+    def reduce(x, op):
+        if pg:
+            t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=op)
+            x = float(t.item())
+        return x
+
+    MAX = pg.ReduceOp.MAX if pg else None
+    SUM = pg.ReduceOp.SUM if pg else None
+    s.upload(evp1d.FieldSet.from_problem(band.local))
+    for _ in range(args.warmup):
+        sweep(ndte)
+    s.synchronize()
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
+    sampler = ClockSampler(gpu_id) if not args.no_clocks else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__enter__()
+    s.launch_count(reset=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sweep(ndte)
+    e1.record(stream)
+    e1.synchronize()
+    launches = s.launch_count()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    t_dev = e0.elapsed_time(e1) / 1000.0
+    t_max = reduce(t_dev, MAX)
+    value = pr.n_active * ndte * args.steps / t_max
+    # end to end: BandSolver.run on page-locked host arrays of the band
+    e2e = []
+    for _ in range(args.e2e_steps):
+        fs_e = evp1d.FieldSet.from_problem(band.local, pinned=True)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        bsol.run(ndte, fs_e)
+        a1.record(stream)
+        a1.synchronize()
+        e2e.append(a0.elapsed_time(a1) / 1000.0)
+    e2e_value = pr.n_active * ndte / reduce(statistics.median(e2e), MAX) if e2e else None
+    h2d, d2h = alg_bytes.host_bytes(band.local)
+    h2d, d2h = reduce(h2d, SUM), reduce(d2h, SUM)
+    sent = reduce(16 * len(band.send_idx()), SUM)
+    ring = reduce(band.local.na - band.n_own, SUM)
+    ab = alg_bytes.per_point_subcycle(s.path)
+    sub_s = t_dev / (args.steps * ndte)
+    achieved = ab * band.local.na / sub_s / 1e9
+    peak, peak_src = alg_bytes.hbm_peak(ROOT)
+    path = s.path
+    bsol.finalize()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC + " (one state split over ranks)", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, reference value ranges)",
+            "config": dict(workload_config(args.config, pr, ndte),
+                           parallelism=f"one state in {world} band(s) of the 1D list, "
+                                       f"one per rank, velocity exchange every subcycle",
+                           ring_points=int(ring), exchange_bytes_per_subcycle=int(sent)),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                         "algorithmic_bytes_per_point_subcycle": ab, "kernel": path,
+                         "note": "rank 0's band (owned and ring points) over its own time"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "host_memory": "page-locked",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches,
+            "clocks": sampler.summary() if sampler else None,
+        }), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
 # --------------------------------------------------------------------------
 # GPU
 # --------------------------------------------------------------------------
@@ -593,6 +712,9 @@ def main():
         return
     if args.config in _synth.ENSEMBLES:
         run_ensemble(args, rank, world, local)
+        return
+    if args.split:
+        run_split(args, rank, world, local)
         return
 
     import numpy as np
