@@ -604,13 +604,7 @@ def run_split(args, rank, world, local):
     bsol = bands.BandSolver(band, ndte=ndte, device=local)
     s = bsol.s
     stream = torch.cuda.ExternalStream(s.stream, device=local)
-
-    def sweep(n):
-        with torch.cuda.stream(stream):
-            bands.run_band(band, n, lambda: s.subcycles(1),
-                           lambda b: s.exchange_pack(b.data_ptr()),
-                           lambda b: s.exchange_unpack(b.data_ptr()),
-                           bsol.send_buf, bsol.recv_buf)
+    sweep = bsol.subcycles
 
     def reduce(x, op):
         if pg:

@@ -177,42 +177,61 @@ def run_band(band: Band, nsub: int, step, pack, unpack, send_buf, recv_buf,
         unpack(recv_buf)
 
 
+class _DeviceArray:
+    """__cuda_array_interface__ of device memory the library owns."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 3}
+
+
+def device_view(ptr: int, n: int, device):
+    """A float64 torch tensor over `n` doubles of device memory at `ptr`
+    (no copy; valid while the owner keeps the memory)."""
+    import torch
+    if n == 0 or not ptr:
+        return torch.zeros(0, dtype=torch.float64, device=device)
+    return torch.as_tensor(_DeviceArray(ptr, n), device=device)
+
+
 class BandSolver:
     """This rank's band on its GPU: an EVP1D handle of the band's local
-    problem with the exchange lists set, and device buffers for the moves.
+    problem with the exchange lists set.  The handle's own exchange buffers
+    (evp1d_exchange_buffers) are what NCCL sends from and receives into.
     ``run`` mirrors EVP1D.run on the band's local FieldSet; all ranks call
     it together (NCCL point-to-point with the neighbouring bands)."""
 
     def __init__(self, band: Band, ndte: int = None, params=None, device: int = 0,
                  group=None):
         import torch
+        import torch.distributed as dist
         from . import EVP1D
         self.band, self.group = band, group
         self.device = torch.device("cuda", device)
         self.s = EVP1D.from_problem(band.local, ndte=ndte, params=params, device=device)
         self.s.exchange_setup(band.send_idx(), band.recv_idx())
-        self.send_buf = torch.empty(2 * len(band.send_idx()), dtype=torch.float64,
-                                    device=self.device)
-        self.recv_buf = torch.empty(2 * len(band.recv_idx()), dtype=torch.float64,
-                                    device=self.device)
-        import torch.distributed as dist
+        ps, pr = self.s.exchange_buffers()
+        self.send_buf = device_view(ps, 2 * len(band.send_idx()), self.device)
+        self.recv_buf = device_view(pr, 2 * len(band.recv_idx()), self.device)
         if dist.is_initialized():
             # NCCL creates its communicator on the first collective, which
             # must involve every rank; a band without neighbours posts no
             # point-to-point operation later
             dist.barrier(group=group)
 
-    def run(self, ndte: int, fields):
+    def subcycles(self, n: int) -> None:
+        """`n` subcycles of the uploaded band, each followed by the exchange,
+        all ordered on the handle's stream."""
         import torch
         s = self.s
-        s.upload(fields)
-        stream = torch.cuda.ExternalStream(s.stream, device=self.device)
-        with torch.cuda.stream(stream):
-            run_band(self.band, ndte, lambda: s.subcycles(1),
-                     lambda b: s.exchange_pack(b.data_ptr()),
-                     lambda b: s.exchange_unpack(b.data_ptr()),
-                     self.send_buf, self.recv_buf, self.group)
-        s.download(fields)
+        with torch.cuda.stream(torch.cuda.ExternalStream(s.stream, device=self.device)):
+            run_band(self.band, n, lambda: s.subcycles(1), lambda b: s.exchange_pack(),
+                     lambda b: s.exchange_unpack(), self.send_buf, self.recv_buf, self.group)
+
+    def run(self, ndte: int, fields):
+        self.s.upload(fields)
+        self.subcycles(ndte)
+        self.s.download(fields)
         return fields
 
     def finalize(self) -> None:
@@ -239,15 +258,13 @@ def time_bands(pr, nbands: int, nsub: int = 200, warmup: int = 5, device: int = 
         s = EVP1D.from_problem(b.local, device=device)
         with s:
             s.exchange_setup(b.send_idx(), b.recv_idx())
-            send = torch.zeros(2 * len(b.send_idx()) + 1, dtype=torch.float64, device=dev)
-            recv = torch.zeros(2 * len(b.recv_idx()) + 1, dtype=torch.float64, device=dev)
             s.upload(FieldSet.from_problem(b.local))
             stream = torch.cuda.ExternalStream(s.stream, device=dev)
 
             def step():
                 s.subcycles(1)
-                s.exchange_pack(send.data_ptr())
-                s.exchange_unpack(recv.data_ptr())
+                s.exchange_pack()
+                s.exchange_unpack()
 
             for _ in range(warmup):
                 step()

@@ -34,20 +34,6 @@ def _outs(fs):
                 strinty=fs.strinty, Cb=fs.Cb)
 
 
-class _DeviceArray:
-    """A library-owned device buffer seen by torch without a copy."""
-
-    def __init__(self, ptr, n):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
-                                         "data": (ptr, False), "version": 3}
-
-
-def _wrap(ptr, n, dev):
-    if n == 0:
-        return torch.zeros(0, dtype=torch.float64, device=dev)
-    return torch.as_tensor(_DeviceArray(ptr, n), device=dev)
-
-
 def solve_bands_one_gpu(pr, nbands, ndte, own_buffers=False):
     """own_buffers: pack into and unpack from the handles' own exchange
     buffers (evp1d_exchange_buffers) instead of caller buffers."""
@@ -66,8 +52,8 @@ def solve_bands_one_gpu(pr, nbands, ndte, own_buffers=False):
             if own_buffers:
                 ps, pr_ = s.exchange_buffers()
                 assert (ps != 0) == (ns > 0) and (pr_ != 0) == (nr > 0)
-                sbuf.append(_wrap(ps, ns, dev))
-                rbuf.append(_wrap(pr_, nr, dev))
+                sbuf.append(B.device_view(ps, ns, dev))
+                rbuf.append(B.device_view(pr_, nr, dev))
             else:
                 sbuf.append(torch.zeros(ns, dtype=torch.float64, device=dev))
                 rbuf.append(torch.zeros(nr, dtype=torch.float64, device=dev))
