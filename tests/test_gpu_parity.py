@@ -364,6 +364,48 @@ def test_batched_ensemble_matches_members(oracle_mod):
         assert_same(one, st, pr)
 
 
+def _empty_member(like):
+    z = np.zeros(0)
+    zi = np.zeros(0, np.int32)
+    return synth.Problem1D(na=0, navel=0, ndte=like.ndte, idx={k: zi.copy() for k in like.idx},
+                           skipT=zi.copy(), skipU=zi.copy(), f={k: z.copy() for k in like.f},
+                           stress=np.zeros((12, 0)), uvel=z.copy(), vvel=z.copy(),
+                           strintx=z.copy(), strinty=z.copy(), Cb=z.copy())
+
+
+def test_batched_ensemble_with_empty_and_one_point_members(oracle_mod):
+    """Members without ice (na = 0: first, in the middle, last) and a member
+    of one point whose neighbours are all halo slots sit beside ordinary
+    members; every member still gets its own result bit for bit."""
+    a = synth.make_problem("grid400x300", nx=40, ny=30, seed=61, ndte=6)
+    b = synth.make_problem("grid400x300", nx=55, ny=25, seed=62, ndte=6)
+    one = helpers.random_graph_problem(1, 6, 3)
+    one.idx = {k: np.array([2 + i], np.int32) for i, k in enumerate(("ee", "ne", "se", "nw", "sw", "sse"))}
+    one.navel = 7
+    one.uvel = np.concatenate([one.uvel[:1], np.zeros(6)])
+    one.vvel = np.concatenate([one.vvel[:1], np.zeros(6)])
+    one.skipT[:] = 0
+    one.skipU[:] = 0
+    one.ndte = 6
+    members = [_empty_member(a), a, _empty_member(a), one, b, _empty_member(a)]
+    ens = synth.concat(members)
+    fs = evp1d.FieldSet.from_problem(ens.combined)
+    with evp1d.EVP1D.batched(ens, ndte=6) as s:
+        s.run(6, fs)
+    for m, pr in enumerate(members):
+        if pr.na == 0:
+            continue
+        st = oracle_run(oracle_mod, pr, 6)
+        got = evp1d.FieldSet(pr.na, pr.navel, skipT=pr.skipT, skipU=pr.skipU,
+                             stress=ens.split_points(fs.stress)[m],
+                             uvel=ens.split_slots(fs.uvel)[m], vvel=ens.split_slots(fs.vvel)[m],
+                             strintx=ens.split_points(fs.strintx)[m],
+                             strinty=ens.split_points(fs.strinty)[m],
+                             Cb=ens.split_points(fs.Cb)[m],
+                             **{k: pr.f[k] for k in evp1d.FieldSet.DYN})
+        assert_same(got, st, pr)
+
+
 def test_autotune_keeps_state(oracle_mod):
     pr = synth.make_problem("grid400x300", nx=120, ny=90, ndte=12)
     fs = evp1d.FieldSet.from_problem(pr, want_str=True)
