@@ -60,6 +60,14 @@ def parse():
     ap.add_argument("--split", action="store_true",
                     help="one state of --config split into one band per rank, with a "
                          "velocity exchange (NCCL) every subcycle: strong scaling")
+    ap.add_argument("--band-timing", type=int, nargs="*", default=None,
+                    help="time the bands of a split of --config into each given number "
+                         "of bands on one GPU (the per-rank compute of such a split)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave out the ensemble and adjoint keys of the default line")
+    ap.add_argument("--extras-ndte", type=int, default=None,
+                    help="subcycles of the ensemble and adjoint keys (default: the "
+                         "configurations' own, 500)")
     return ap.parse_args()
 
 
@@ -689,6 +697,228 @@ def run_split(args, rank, world, local):
 
 
 # --------------------------------------------------------------------------
+# GPU: the ensemble and adjoint keys of the default line
+# --------------------------------------------------------------------------
+def _event_pair():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def ensemble_extras(local: int, steps: int, ndte: int = None) -> dict:
+    """The 64-member ensemble (ens64): one batched handle against looping one
+    handle per member, all CUDA-event timed on the device.
+
+    - batched: evp1d_subcycles(ndte) of the batched handle.
+    - serial loop: member after member, each evp1d_subcycles(ndte) followed by
+      a synchronize before the next member starts (the loop a host code
+      runs); the members' device times summed.
+    - concurrent loop: every member issued at once, each on its own handle's
+      stream; from an event all the streams wait on to an event that waits
+      on all of them.
+    - equal: one call of ndte from the same starting state, every output
+      array of every member bit for bit between the batched handle and the
+      serial loop."""
+    import numpy as np
+    import torch
+    import evp1d
+    from evp1d import synth
+
+    cfg = dict(synth.ENSEMBLES["ens64"])
+    if ndte:
+        cfg["ndte"] = ndte
+    ndte = cfg["ndte"]
+    members = synth.make_ensemble(**cfg)
+    ens = synth.concat(members)
+    units = sum(m.n_active for m in members) * ndte
+    dev = torch.device("cuda", local)
+
+    # batched
+    fb = evp1d.FieldSet.from_problem(ens.combined)
+    s = evp1d.EVP1D.batched(ens, ndte=ndte, device=local)
+    st_b = torch.cuda.ExternalStream(s.stream, device=dev)
+    s.upload(fb)
+    s.subcycles(ndte)
+    s.synchronize()
+    t_b = []
+    for _ in range(steps):
+        e0, e1 = _event_pair()
+        e0.record(st_b)
+        s.subcycles(ndte)
+        e1.record(st_b)
+        e1.synchronize()
+        t_b.append(e0.elapsed_time(e1) / 1000.0)
+    # equality pass, from the starting state
+    fb = evp1d.FieldSet.from_problem(ens.combined)
+    s.run(ndte, fb)
+    s.finalize()
+
+    handles, streams = [], []
+    for m in members:
+        h = evp1d.EVP1D.from_problem(m, ndte=ndte, device=local)
+        handles.append(h)
+        streams.append(torch.cuda.ExternalStream(h.stream, device=dev))
+    equal = True
+    off = 0
+    us, vs = ens.split_slots(fb.uvel), ens.split_slots(fb.vvel)
+    for i, (m, h) in enumerate(zip(members, handles)):
+        fm = evp1d.FieldSet.from_problem(m)
+        h.run(ndte, fm)
+        sl = slice(off, off + m.na)
+        pairs = ((fb.stress[:, sl], fm.stress), (us[i][: m.na], fm.uvel[: m.na]),
+                 (vs[i][: m.na], fm.vvel[: m.na]), (fb.strintx[sl], fm.strintx),
+                 (fb.strinty[sl], fm.strinty), (fb.Cb[sl], fm.Cb))
+        for a, b in pairs:
+            equal &= bool(np.array_equal(np.ascontiguousarray(a).view(np.int64),
+                                         np.ascontiguousarray(b).view(np.int64)))
+        off += m.na
+        h.upload(evp1d.FieldSet.from_problem(m))
+        h.subcycles(ndte)
+        h.synchronize()
+
+    # serial loop
+    t_s = []
+    for _ in range(steps):
+        tot = 0.0
+        for h, st in zip(handles, streams):
+            e0, e1 = _event_pair()
+            e0.record(st)
+            h.subcycles(ndte)
+            e1.record(st)
+            h.synchronize()
+            tot += e0.elapsed_time(e1) / 1000.0
+        t_s.append(tot)
+    # concurrent loop
+    side = torch.cuda.Stream(device=dev)
+    t_c = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0, e1 = _event_pair()
+        e0.record(side)
+        ends = []
+        for h, st in zip(handles, streams):
+            st.wait_event(e0)
+            h.subcycles(ndte)
+            e = torch.cuda.Event()
+            e.record(st)
+            ends.append(e)
+        for e in ends:
+            side.wait_event(e)
+        e1.record(side)
+        e1.synchronize()
+        t_c.append(e0.elapsed_time(e1) / 1000.0)
+    for h in handles:
+        h.finalize()
+    med = statistics.median
+    b, sl_, co = units / med(t_b), units / med(t_s), units / med(t_c)
+    return {"config": "ens64", "members": len(members), "active_points": units // ndte,
+            "ndte": ndte, "steps": steps,
+            "batched": b, "serial_loop": sl_, "concurrent_loop": co, "unit": UNIT,
+            "batched_over_serial_loop": b / sl_, "batched_over_concurrent_loop": b / co,
+            "ms": {"batched": 1000 * med(t_b), "serial_loop": 1000 * med(t_s),
+                   "concurrent_loop": 1000 * med(t_c)},
+            "equal_bitwise_per_member": equal,
+            "timing": "CUDA events on the device; serial loop = sum of the members' "
+                      "device times, one member at a time"}
+
+
+def adjoint_extras(local: int, steps: int, ndte: int = None) -> dict:
+    """The single-problem adjoint (adjoint800x600: J = misfit of the final
+    velocities, gradients with respect to strength, Cw, forcex, forcey):
+    forward, recording forward and reverse sweep, CUDA-event timed, with
+    checkpoints every 50 subcycles and with the checkpointing sized to device
+    memory.  The cost of a gradient is (record + sweep) / forward."""
+    import torch
+    import evp1d
+    from evp1d import synth
+
+    over = {"ndte": ndte} if ndte else {}
+    pr = synth.make_problem("adjoint800x600", **over)
+    ndte = pr.ndte
+    uobs, vobs = synth.observations(pr.na, seed=synth.CONFIGS["adjoint800x600"]["seed"] + 500)
+    interval = synth.ADJOINT_INTERVAL
+    fs = evp1d.FieldSet.from_problem(pr)
+    s = evp1d.EVP1D.from_problem(pr, ndte=ndte, device=local)
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
+    s.run(ndte, fs)
+    lam = _misfit_seed(fs.uvel[: pr.na], fs.vvel[: pr.na], uobs, vobs)
+    fields = lambda: evp1d.FieldSet.from_problem(pr)
+    s.upload(fields())
+    s.subcycles(ndte)
+    _adjoint_once(s, stream, ndte, interval, lam, fields)
+    _adjoint_once(s, stream, ndte, 0, lam, fields)
+    t_f, t_r, t_w, t_r0, t_w0 = [], [], [], [], []
+    for _ in range(steps):
+        s.upload(fields())
+        t_f.append(_timed(stream, lambda: s.subcycles(ndte)))
+        a, b = _adjoint_once(s, stream, ndte, interval, lam, fields)
+        t_r.append(a)
+        t_w.append(b)
+        a, b = _adjoint_once(s, stream, ndte, 0, lam, fields)
+        t_r0.append(a)
+        t_w0.append(b)
+    info0 = s.adjoint_info()
+    s.finalize()
+    med = statistics.median
+    f = med(t_f)
+    return {"config": "adjoint800x600", "active_points": pr.n_active, "ndte": ndte,
+            "steps": steps, "forward_ms": 1000 * f,
+            "every_50": {"record_ms": 1000 * med(t_r), "sweep_ms": 1000 * med(t_w),
+                         "gradient_over_forward": (med(t_r) + med(t_w)) / f,
+                         "sweep_over_forward": med(t_w) / f},
+            "memory_sized": {"record_ms": 1000 * med(t_r0), "sweep_ms": 1000 * med(t_w0),
+                             "gradient_over_forward": (med(t_r0) + med(t_w0)) / f,
+                             "tape_subcycles": info0["tape_subcycles"],
+                             "interval": info0["interval"]},
+            "timing": "CUDA events on the solver's stream"}
+
+
+def run_band_timing(args, local):
+    """--band-timing K...: the per-rank work of a split of --config into K
+    bands, measured on one GPU.  Each band's handle runs 200 steps of (one
+    subcycle, pack, unpack) on its own stream, timed with CUDA events on that
+    stream; the exchange between GPUs (NCCL) is not part of it.  One JSON line
+    per K: microseconds per step of every band and the bytes each band sends
+    per subcycle."""
+    import torch
+    import evp1d
+    from evp1d import synth, bands
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pr = synth.make_problem(args.config)
+    nsub, warmup = 200, 5
+    for nb in (args.band_timing or [1, 2, 4, 8]):
+        out = dict(problem=args.config, na=pr.na, nbands=nb, us=[], points=[], ring=[],
+                   send_bytes=[])
+        for b in bands.split(pr, nb):
+            with evp1d.EVP1D.from_problem(b.local, device=local) as s:
+                s.exchange_setup(b.send_idx(), b.recv_idx())
+                s.upload(evp1d.FieldSet.from_problem(b.local))
+                stream = torch.cuda.ExternalStream(s.stream, device=dev)
+
+                def step():
+                    s.subcycles(1)
+                    s.exchange_pack()
+                    s.exchange_unpack()
+
+                for _ in range(warmup):
+                    step()
+                s.synchronize()
+                e0, e1 = _event_pair()
+                e0.record(stream)
+                for _ in range(nsub):
+                    step()
+                e1.record(stream)
+                e1.synchronize()
+                out["us"].append(1000.0 * e0.elapsed_time(e1) / nsub)
+                out["points"].append(b.n_own)
+                out["ring"].append(b.local.na - b.n_own)
+                out["send_bytes"].append(16 * len(b.send_idx()))
+        out["max_us"] = max(out["us"])
+        print(json.dumps(out), flush=True)
+
+
+# --------------------------------------------------------------------------
 # GPU
 # --------------------------------------------------------------------------
 def main():
@@ -709,6 +939,10 @@ def main():
         return
     if args.split:
         run_split(args, rank, world, local)
+        return
+    if args.band_timing is not None:
+        if rank == 0:
+            run_band_timing(args, local)
         return
 
     import numpy as np
@@ -855,6 +1089,10 @@ def main():
 
     path = solver.path
     solver.finalize()
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["ensemble"] = ensemble_extras(local, 2, args.extras_ndte)
+        extras["adjoint"] = adjoint_extras(local, 2, args.extras_ndte)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -884,6 +1122,7 @@ def main():
             "lindividual": lind,
             "cpu_baseline": cpu,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()

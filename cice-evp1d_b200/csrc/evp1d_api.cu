@@ -173,8 +173,18 @@ int evp1d_host_free(void *ptr) {
   return EVP1D_OK;
 }
 
+#ifndef EVP_TARGET
+#define EVP_TARGET "unknown target"
+#endif
 const char *evp1d_version(void) {
-  return "evp1d-b200 0.2 (sm_100a, fp64, fused tile solver)";
+  return "evp1d-b200 0.3 (" EVP_TARGET ", fp64, fused tile solver)";
+}
+
+int evp1d_binary_version(int device) {
+  CUDA_TRY(cudaSetDevice(device));
+  int v = 0;
+  CUDA_TRY(evp::tma_binary_version(&v));
+  return v;
 }
 
 void evp1d_set_evp_parameters(evp1d_params *p, int ndte) {
@@ -627,11 +637,17 @@ int evp1d_autotune(evp1d_t *h, int nsub, char *chosen, int len) {
     h->prefetch = cands[c].prefetch;
     drop_graphs(h);
     rc = evp1d_subcycles(h, 2);  // warm-up (also builds nothing: < one chunk)
-    if (rc != EVP1D_OK) break;
-    cudaEventRecord(e0, st);
-    rc = evp1d_subcycles(h, nsub);
-    cudaEventRecord(e1, st);
-    if (rc != EVP1D_OK) break;
+    if (rc == EVP1D_OK) {
+      cudaEventRecord(e0, st);
+      rc = evp1d_subcycles(h, nsub);
+      cudaEventRecord(e1, st);
+    }
+    if (rc != EVP1D_OK) {
+      // put the caller's state back before reporting the failed trial
+      copy_all(false);
+      d.cur = cur0;
+      break;
+    }
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);

@@ -116,6 +116,8 @@ constexpr int kTraceTiles = 256;
 
 // Allow the kernel's dynamic shared memory (call once per device).
 int tma_prepare(int device);
+// binaryVersion of the subcycle kernel on the current device (100 = sm_100a).
+cudaError_t tma_binary_version(int *version);
 // What the wait that left `code` in the error word was waiting for.
 const char *tma_wait_name(int code);
 // One bounded wait on an mbarrier that nothing completes: it runs out after

@@ -7,7 +7,7 @@
 //   - the stress part (geometry, strength, packed index words, the 12
 //     stresses, u and v of the owned points and of the stencil's extra
 //     points, and the recomputed forward halo) is dead once stress is done;
-//     it has a three-slot ring, so two later tiles load while one computes;
+//     it has a two-slot ring, so one later tile loads while one computes;
 //   - the stepu part (the 13 stepu inputs) has one slot, loaded while the
 //     consumers compute the tile's stress.
 // The owned points of a tile are contiguous slots and its per-call constants
@@ -591,6 +591,13 @@ const char *tma_wait_name(int code) {
     case kProbeCode: return "the wait probe (evp1d_debug_wait_timeout)";
     default: return "unknown";
   }
+}
+
+cudaError_t tma_binary_version(int *version) {
+  cudaFuncAttributes at;
+  const cudaError_t e = cudaFuncGetAttributes(&at, k_tma<false, true>);
+  if (e == cudaSuccess) *version = at.binaryVersion;
+  return e;
 }
 
 void launch_wait_probe(int *err, unsigned long long limit_ns, cudaStream_t st) {

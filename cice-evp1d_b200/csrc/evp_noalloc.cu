@@ -9,7 +9,6 @@
 // The only scratch -- str1..str8 and the velocities at call start -- lives in
 // one file-scope device array of fixed size, so the call allocates nothing.
 #include <cstdint>
-#include <mutex>
 
 #include "evp1d.h"
 #include "evp_internal.h"
@@ -23,15 +22,13 @@ constexpr int kThreads = 256;
 // start, vvel at call start, each kNoAllocMaxNavel doubles (20 MiB in all).
 constexpr int kNoAllocMaxNavel = EVP1D_NOALLOC_MAX_NAVEL;
 constexpr int kScratchArrays = 10;
+// The check's "no bad neighbour" value: every byte 0x7f (one cudaMemsetAsync),
+// above any 1 + point index since navel <= kNoAllocMaxNavel.
+constexpr int kStatusNone = 0x7f7f7f7f;
 
 static __device__ __align__(256) double g_scratch[kScratchArrays * (size_t)kNoAllocMaxNavel];
 // Index-check result of the current call (0 = every neighbour in range).
 static __device__ __align__(256) int g_status[1];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-double *g_scratch_ptr[kMaxDevices] = {};
-int *g_status_ptr[kMaxDevices] = {};
 
 struct NaArgs {
   int na, navel;
@@ -47,7 +44,8 @@ struct NaArgs {
   double *strintx, *strinty, *Cb;
 };
 
-// Flags any neighbour outside 1..navel (status[0] = 1 + first bad point).
+// Flags any neighbour outside 1..navel: status[0], which starts at
+// kStatusNone, ends as 1 + the lowest 0-based point with a bad neighbour.
 __global__ void __launch_bounds__(kThreads) k_na_check(NaArgs a, int *status) {
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < a.na;
        w += gridDim.x * blockDim.x) {
@@ -58,7 +56,7 @@ __global__ void __launch_bounds__(kThreads) k_na_check(NaArgs a, int *status) {
       const int32_t x = nb[k][w];
       bad |= x < 1 || x > a.navel;
     }
-    if (bad) atomicCAS(status, 0, w + 1);
+    if (bad) atomicMin(status, w + 1);
   }
 }
 
@@ -136,21 +134,17 @@ __global__ void __launch_bounds__(kThreads) k_na_stepu(NaArgs a, Params p) {
       return error(EVP1D_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_));  \
   } while (0)
 
-// Device addresses of the scratch on the current device, looked up on the
-// first call made with that device current.
-int scratch_for_device(int dev, double **scratch, int **status) {
-  if (dev < 0 || dev >= kMaxDevices)
-    return error(EVP1D_ERR_INVALID_ARG, "device %d out of range", dev);
-  std::lock_guard<std::mutex> lk(g_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void *ps = nullptr, *pe = nullptr;
-    NA_TRY(cudaGetSymbolAddress(&ps, g_scratch));
-    NA_TRY(cudaGetSymbolAddress(&pe, g_status));
-    g_scratch_ptr[dev] = static_cast<double *>(ps);
-    g_status_ptr[dev] = static_cast<int *>(pe);
-  }
-  *scratch = g_scratch_ptr[dev];
-  *status = g_status_ptr[dev];
+// Device addresses of the scratch in the current context.  Looked up on
+// every call: the module holding the arrays is loaded once per context, so
+// after a cudaDeviceReset, or in a context other than the primary one, the
+// arrays can sit at another address than in an earlier call.  The lookup
+// allocates nothing once the module is loaded.
+int scratch_in_context(double **scratch, int **status) {
+  void *ps = nullptr, *pe = nullptr;
+  NA_TRY(cudaGetSymbolAddress(&ps, g_scratch));
+  NA_TRY(cudaGetSymbolAddress(&pe, g_status));
+  *scratch = static_cast<double *>(ps);
+  *status = static_cast<int *>(pe);
   return EVP1D_OK;
 }
 
@@ -220,7 +214,7 @@ extern "C" int evp1d_run_device_noalloc(int na, int navel, const int32_t *ee,
   NA_TRY(cudaGetDevice(&dev));
   double *scratch = nullptr;
   int *status = nullptr;
-  int rc = scratch_for_device(dev, &scratch, &status);
+  int rc = scratch_in_context(&scratch, &status);
   if (rc != EVP1D_OK) return rc;
   if (na == 0 || ndte == 0) return EVP1D_OK;
 
@@ -299,14 +293,15 @@ extern "C" int evp1d_run_device_noalloc(int na, int navel, const int32_t *ee,
   }
 
   // neighbour check before any state is touched
-  int host_status = 0;
-  NA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
+  int host_status = kStatusNone;
+  NA_TRY(cudaMemsetAsync(status, 0x7f, sizeof(int), st));
   k_na_check<<<grid_for(na), kThreads, 0, st>>>(a, status);
   NA_TRY(cudaGetLastError());
   NA_TRY(cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st));
   NA_TRY(cudaStreamSynchronize(st));
-  if (host_status != 0)
-    return error(EVP1D_ERR_INDEX, "neighbour of point %d (1-based) outside 1..navel=%d",
+  if (host_status != kStatusNone)
+    return error(EVP1D_ERR_INDEX,
+                 "point %d (1-based) is the first with a neighbour outside 1..navel=%d",
                  host_status, navel);
 
   // str1..str8 start at zero on every call: stepu reads them at halo slots

@@ -100,6 +100,8 @@ def load() -> C.CDLL:
     L.evp1d_last_error.restype = C.c_char_p
     L.evp1d_last_error.argtypes = []
     L.evp1d_version.restype = C.c_char_p
+    L.evp1d_binary_version.argtypes = [C.c_int]
+    L.evp1d_binary_version.restype = C.c_int
     L.evp1d_init_batched.argtypes = ([C.POINTER(H), C.c_int, _I, _I] + [_I] * 6
                                      + [_D] * 7 + [C.POINTER(Params), C.c_int])
     L.evp1d_init_batched.restype = C.c_int

@@ -242,63 +242,3 @@ class BandSolver:
 
     def __exit__(self, *exc):
         self.finalize()
-
-
-def time_bands(pr, nbands: int, nsub: int = 200, warmup: int = 5, device: int = 0) -> dict:
-    """The per-rank work of a split into `nbands`, measured on one GPU: each
-    band's handle runs `nsub` steps of (one subcycle, pack, unpack) on its
-    own stream, timed with CUDA events on that stream.  The exchange itself
-    (NCCL between GPUs) is not part of it.  Returns microseconds per step
-    for every band, and the bytes each band sends per subcycle."""
-    import torch
-    from . import EVP1D, FieldSet
-    dev = torch.device("cuda", device)
-    out = dict(nbands=nbands, us=[], points=[], ring=[], send_bytes=[])
-    for b in split(pr, nbands):
-        s = EVP1D.from_problem(b.local, device=device)
-        with s:
-            s.exchange_setup(b.send_idx(), b.recv_idx())
-            s.upload(FieldSet.from_problem(b.local))
-            stream = torch.cuda.ExternalStream(s.stream, device=dev)
-
-            def step():
-                s.subcycles(1)
-                s.exchange_pack()
-                s.exchange_unpack()
-
-            for _ in range(warmup):
-                step()
-            s.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(nsub):
-                step()
-            e1.record(stream)
-            e1.synchronize()
-            out["us"].append(1000.0 * e0.elapsed_time(e1) / nsub)
-            out["points"].append(b.n_own)
-            out["ring"].append(b.local.na - b.n_own)
-            out["send_bytes"].append(16 * len(b.send_idx()))
-    return out
-
-
-def _main(argv=None) -> int:
-    import argparse
-    import json
-    from . import synth
-    ap = argparse.ArgumentParser(description="Time the bands of a split state on one GPU "
-                                 "(the per-rank compute of a split over that many GPUs).")
-    ap.add_argument("--problem", default="grid1600x1200", choices=sorted(synth.CONFIGS))
-    ap.add_argument("--bands", type=int, nargs="+", default=[1, 2, 4, 8])
-    ap.add_argument("--nsub", type=int, default=200)
-    a = ap.parse_args(argv)
-    pr = synth.make_problem(a.problem)
-    for k in a.bands:
-        r = time_bands(pr, k, nsub=a.nsub)
-        print(json.dumps(dict(problem=a.problem, na=pr.na, **r, max_us=max(r["us"]))), flush=True)
-    return 0
-
-
-if __name__ == "__main__":
-    raise SystemExit(_main())

@@ -56,7 +56,9 @@ def host_bytes(pr) -> tuple:
     """Bytes copied host->device and device->host by one evp1d_run call with
     uvel_init/vvel_init defaulted and str not requested."""
     na, navel = pr.na, pr.navel
-    h2d = na * 1 + 8 * na * (12 + 12 + 3) + 8 * navel * 2
+    # skipT and skipU as two int32 arrays, 12 inputs, 12 stresses, strintx,
+    # strinty, Cb over the list points, uvel and vvel with their halo slots
+    h2d = 4 * na * 2 + 8 * na * (12 + 12 + 3) + 8 * navel * 2
     d2h = 8 * na * (12 + 2 + 3)
     return h2d, d2h
 

@@ -202,8 +202,14 @@ long long evp1d_launch_count(evp1d_t *handle, int reset);
 /* Message of the last error on this host thread ("" if none). */
 const char *evp1d_last_error(void);
 
-/* Library version string. */
+/* Library version string; it names the GPU target the library was compiled
+ * for ("sm_100a"). */
 const char *evp1d_version(void);
+
+/* The compute capability the subcycle kernel's code was compiled for, as the
+ * CUDA runtime reports it for `device` (major*10 + minor, 100 for sm_100a),
+ * or a negative EVP1D_ERR_* code. */
+int evp1d_binary_version(int device);
 
 /* Page-locked (pinned) host memory for the arrays of evp1d_fields and
  * evp1d_grads.  Copies from and to it run at full host-link speed and are
@@ -417,8 +423,11 @@ int evp1d_adjoint_info(evp1d_t *handle, long long info[8]);
  * - str1..str8 are cleared at the start of every call.  Every call on a
  *   device shares that array, so calls that overlap on the GPU (from several
  *   host threads, or on streams that run concurrently) race; serialise them.
- * - The first call with a device current looks up the array's device
- *   address; make that first call before any stream capture.
+ * - Every call looks up the array's device address in the current context
+ *   (a lookup that allocates nothing), so a cudaDeviceReset or a context of
+ *   the caller's own between calls is safe.  The call synchronises
+ *   `stream` (it reads the index check back), so it cannot be captured
+ *   into a CUDA graph.
  * - Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
  *   stream) and the call returns after the stream has finished it.
  *   Neighbours outside 1..navel give EVP1D_ERR_INDEX before any array is

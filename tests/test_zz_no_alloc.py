@@ -109,6 +109,39 @@ def test_two_calls_match_evp1d_run(explicit_init):
     assert not np.array_equal(fs.stress, pr.stress)
 
 
+@pytest.mark.parametrize("explicit_init", [False, True])
+def test_two_calls_match_the_oracle(oracle_mod, explicit_init):
+    """The same two calls against the CPU oracle directly, bit for bit, with
+    both reference output files md5-equal after each call."""
+    from test_gpu_parity import assert_same, oracle_run
+    pr = synth.make_problem("grid400x300", nx=140, ny=100, ndte=23)
+    assert pr.navel <= MAX_NAVEL
+    ndte = pr.ndte
+    params = evp1d.set_evp_parameters(ndte)
+    dc = DeviceCase(pr, explicit_init=explicit_init)
+    cur = pr.copy()
+    for call in range(2):
+        _lib.check(dc.run(ndte, params), "evp1d_run_device_noalloc")
+        st = oracle_run(oracle_mod, cur, ndte)
+        got = dc.host()
+        fs = evp1d.FieldSet.from_problem(cur, want_str=True)
+        fs.stress[:], fs.strintx[:], fs.strinty[:], fs.Cb[:] = (
+            got["stress"], got["strintx"], got["strinty"], got["Cb"])
+        fs.uvel[:], fs.vvel[:], fs.str[:] = got["uvel"], got["vvel"], got["str"]
+        assert_same(fs, st, cur)
+        # the next call starts from this one's state; without explicit
+        # uvel_init it also starts its uvel_init there
+        cur = cur.copy()
+        cur.stress[:] = st.stress
+        cur.uvel[:] = st.uvel[: pr.navel]
+        cur.vvel[:] = st.vvel[: pr.navel]
+        cur.strintx[:], cur.strinty[:], cur.Cb[:] = st.strintx, st.strinty, st.Cb
+        if not explicit_init:
+            cur.f["uvel_init"] = st.uvel[: pr.na].copy()
+            cur.f["vvel_init"] = st.vvel[: pr.na].copy()
+    assert not np.array_equal(cur.uvel[: pr.na], pr.uvel[: pr.na])
+
+
 def test_other_sizes_between_calls():
     """A smaller problem after a larger one: the shared scratch is cleared."""
     big = synth.make_problem("grid400x300", nx=90, ny=70, ndte=6)
