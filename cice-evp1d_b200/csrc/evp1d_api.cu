@@ -1,5 +1,6 @@
 // evp1d_api.cu -- the C-ABI of include/evp1d.h: handle, validation, host<->
 // device movement and the graph-launched subcycle loop.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -108,7 +109,7 @@ void launch_sub(evp1d_t *h, int from, bool last) {
     evp::TmaArgs a = evp::problem_tma_args(h->d, from);
     a.prefetch = h->prefetch;
     a.trace = h->trace;
-    evp::launch_tma(a, h->p, last, h->d.nctas, h->d.stream);
+    evp::launch_tma(a, h->p, last, h->d.stream);
   } else {
     evp::launch_fused(evp::problem_fused_args(h->d, from), h->p, last, h->d.stream);
   }
@@ -229,9 +230,21 @@ int check_device(int device) {
   return EVP1D_OK;
 }
 
-// Largest tile (points) of the plans of handles created from now on
-// (evp1d_set_tile_points).
-std::atomic<int> g_tile_points{evp::kTileOwned};
+// Largest tile compute set (points) of the plans of handles created from now
+// on (evp1d_set_tile_points).
+std::atomic<int> g_tile_points{evp::kTileCompute};
+
+// Strip width of the grid order: EVP1D_STRIP_W (1..128), else the default.
+int strip_width() {
+  if (const char *e = getenv("EVP1D_STRIP_W")) {
+    const int v = atoi(e);
+    if (v >= 1 && v <= 128) return v;
+  }
+  return evp::kStripWidth;
+}
+
+// Runs (CTAs) of the plans made without a device: the B200's SM count.
+constexpr int kDefaultRuns = 148;
 
 // Validated 1-based neighbour vectors -> tile plan -> device problem.
 int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6],
@@ -243,8 +256,16 @@ int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6]
     for (int w = 0; w < na; w++) nb0[(size_t)k * na + w] = idx[k][w] - 1;
     nbp[k] = nb0.data() + (size_t)k * na;
   }
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  // EVP1D_RUNS (1..SM count): fewer CTAs, for tests of the run boundaries
+  if (const char *e = getenv("EVP1D_RUNS")) {
+    const int v = atoi(e);
+    if (v >= 1 && v < sms) sms = v;
+  }
   evp::TilePlan plan;
-  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, g_tile_points.load());
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, g_tile_points.load(), sms,
+                       strip_width());
   if (getenv("EVP1D_CHECK_PLAN")) {
     std::string first;
     const long long bad = evp::verify_tile_plan(plan, nbp, g_tile_points.load(), &first);
@@ -551,9 +572,9 @@ int evp1d_synchronize(evp1d_t *h) {
 }
 
 int evp1d_set_tile_points(int points) {
-  if (points < 32 || points > evp::kTileOwned)
+  if (points < 32 || points > evp::kTileCompute)
     return fail(EVP1D_ERR_INVALID_ARG, "tile points %d outside [32, %d]", points,
-                evp::kTileOwned);
+                evp::kTileCompute);
   g_tile_points.store(points);
   return EVP1D_OK;
 }
@@ -705,7 +726,8 @@ int plan_from_vectors(int na, int navel, const int32_t *const idx[6], std::vecto
     }
     nbp[k] = nb0.data() + (size_t)k * na;
   }
-  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, plan, g_tile_points.load());
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, plan, g_tile_points.load(),
+                       kDefaultRuns, strip_width());
   return EVP1D_OK;
 }
 }  // namespace
@@ -735,12 +757,14 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
   const int32_t *nbp[6] = {};
   evp::TilePlan plan;
   CHECK(plan_from_vectors(na, navel, idx, nb0, nbp, &plan));
-  long long hmax = 0, tmax = 0, xmax = 0;
+  long long hmax = 0, tmax = 0, xmax = 0, rmax = 0;
   for (int t = 0; t < plan.ntiles; t++) {
     if (plan.halo_cnt[t] > hmax) hmax = plan.halo_cnt[t];
     if (plan.tile_cnt[t] > tmax) tmax = plan.tile_cnt[t];
     if (plan.uvx_cnt[t] > xmax) xmax = plan.uvx_cnt[t];
   }
+  for (int r = 0; r < plan.nruns; r++)
+    rmax = std::max<long long>(rmax, plan.run_off[r + 1] - plan.run_off[r]);
   for (int k = 0; k < 8; k++) stats[k] = 0;
   stats[0] = plan.ntiles;
   stats[1] = plan.nslots;
@@ -749,6 +773,7 @@ int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
   stats[4] = hmax;
   stats[5] = tmax;
   stats[6] = xmax;
+  stats[7] = rmax;
   return EVP1D_OK;
 }
 

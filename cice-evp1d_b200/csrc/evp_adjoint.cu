@@ -469,7 +469,7 @@ void launch_state(evp1d_t *h, double *const s_in[12], double *const s_out[12],
     a.v_in = v_in;
     a.u_out = u_out;
     a.v_out = v_out;
-    launch_tma(a, h->p, last, d.nctas, d.stream);
+    launch_tma(a, h->p, last, d.stream);
   } else {
     FusedArgs a = problem_fused_args(d, 0);
     for (int k = 0; k < 12; k++) {

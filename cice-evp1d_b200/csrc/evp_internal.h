@@ -52,6 +52,8 @@ struct DeviceProblem {
   void *arena = nullptr;
   size_t arena_bytes = 0;
   // tile plan
+  int nruns = 0;                 // CTAs of the subcycle kernel
+  int32_t *run_off = nullptr;    // [nruns + 1] tile ranges of the runs
   int32_t *tile_off = nullptr, *tile_cnt = nullptr, *halo_off = nullptr;
   int32_t *halo_cnt = nullptr, *halo_idx = nullptr;
   int32_t *slot_of_point = nullptr, *point_of_slot = nullptr;
@@ -65,7 +67,7 @@ struct DeviceProblem {
   int32_t *tile_rec = nullptr;   // kRecInts int32 per tile (producer records)
   double *cblk = nullptr;        // per-call constants, kConstFields x 256 per tile
   int *err = nullptr;        // device error word of the bounded waits
-  int nctas = 0;             // persistent grid size (SM count)
+  int nctas = 0;             // SM count of the device
   uint8_t *flags = nullptr;
   double *geo[kNumGeo] = {};
   double *dyn[kNumDyn] = {};

@@ -42,9 +42,12 @@ void launch_stepu(const DevState &s, const Params &p, cudaStream_t st);
 
 // One subcycle of the fused tile solver: stress on every tile's owned points
 // and forward halo, str in shared memory, stepu on the owned points.  Reads
-// the *_in state and writes the *_out state (ping-pong buffers).
+// the *_in state and writes the *_out state (ping-pong buffers).  CTA r works
+// through the tiles of run r in order (a stepu str index may point into the
+// previous tile's table).
 struct FusedArgs {
-  int ntiles = 0;
+  int ntiles = 0, nruns = 0;
+  const int32_t *run_off = nullptr;  // [nruns + 1]
   const int32_t *tile_off = nullptr, *tile_cnt = nullptr;
   const int32_t *halo_off = nullptr, *halo_cnt = nullptr, *halo_idx = nullptr;
   const uint8_t *flags = nullptr;
@@ -86,7 +89,8 @@ constexpr int kConstStressFields = 8;
 constexpr int kConstFields = kConstStressFields + kTmaStepuFields;
 constexpr int kConstTileSlots = kTileOwned;
 struct TmaArgs {
-  int ntiles = 0;
+  int ntiles = 0, nruns = 0;
+  const int32_t *run_off = nullptr;  // [nruns + 1]: CTA r's tiles
   const int32_t *tile_off = nullptr, *tile_cnt = nullptr;
   const int32_t *halo_off = nullptr, *halo_cnt = nullptr, *halo_idx = nullptr;
   const int32_t *uvx_off = nullptr, *uvx_cnt = nullptr, *uvx_idx = nullptr;
@@ -123,8 +127,8 @@ const char *tma_wait_name(int code);
 // One bounded wait on an mbarrier that nothing completes: it runs out after
 // limit_ns and leaves its code in *err (a check of the timeout path).
 void launch_wait_probe(int *err, unsigned long long limit_ns, cudaStream_t st);
-void launch_tma(const TmaArgs &a, const Params &p, bool last, int nctas,
-                cudaStream_t st);
+// One CTA per run (grid = nruns, at most one per SM).
+void launch_tma(const TmaArgs &a, const Params &p, bool last, cudaStream_t st);
 
 // ---- layout conversion between the reference 1D order and slots ----------
 constexpr int kMaxBatch = 32;

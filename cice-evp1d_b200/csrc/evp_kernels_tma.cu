@@ -1,9 +1,9 @@
 // evp_kernels_tma.cu -- the fused EVP subcycle as a persistent, TMA-fed
 // producer/consumer kernel (sm_100a).
 //
-// One CTA per SM walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
-// A tile's inputs are staged in shared memory in two parts with different
-// lifetimes:
+// CTA b works through the tiles of its run, t = run_off[b] .. run_off[b+1]-1,
+// in order (one CTA per SM).  A tile's inputs are staged in shared memory in
+// two parts with different lifetimes:
 //   - the stress part (geometry, strength, packed index words, the 12
 //     stresses, u and v of the owned points and of the stencil's extra
 //     points, and the recomputed forward halo) is dead once stress is done;
@@ -20,10 +20,13 @@
 // tile's slot range and gather lists -- are one 1.3 KB record per tile that a
 // bulk copy brings kRecRing tiles ahead, so no producer waits on a global
 // load.
-// Ten consumer warps (one thread per compute-set point: 256 owned + 64 halo)
-// compute stress from shared memory into the shared str table, then stepu for
-// the owned points, writing the new stresses and velocities to the other
-// ping-pong buffer.
+// Eight consumer warps (one thread per compute-set point: the tile's owned
+// points, then its forward halo, 256 at most) compute stress from shared
+// memory into the tile's str table, then stepu for the owned points, writing
+// the new stresses and velocities to the other ping-pong buffer.  Stepu reads
+// str from the tile's own table and from the previous tile's, which stays
+// alive: three str tables rotate, so that one tile's stress can start while
+// stepu still reads the two before it.
 //
 // Every mbarrier wait is bounded by %globaltimer (kWaitNs): on expiry the
 // kernel records an error code, every thread of the consumer group leaves the
@@ -40,7 +43,7 @@ namespace {
 
 constexpr int kSSlots = 2;                          // stress-part ring
 constexpr int kRecRing = 4;                         // producer records in flight
-constexpr int kConsumers = kTileOwned + kTileHalo;  // 320 = 10 warps
+constexpr int kConsumers = kTileCompute;            // 256 = 8 warps, two per scheduler
 constexpr int kGatherWarps = 2;                     // producer warps issuing cp.async gathers
 constexpr int kStageWarps = 1 + kGatherWarps;       // bulk warp + gather warps
 constexpr int kThreads = kConsumers + 32 * kStageWarps;
@@ -71,7 +74,7 @@ static_assert(kConstFields == kConstStressFields + kTmaStepuFields, "constant bl
 struct Smem {
   SSlot ss[kSSlots];
   USlot us;
-  double str[2][8][kZeroSlot + 2];  // double-buffered str table
+  double str[3][8][kStrRow];  // rotating str tables; position kZeroSlot holds 0
   int32_t rec[kRecRing][kRecInts];
   unsigned long long sfull[kSSlots];
   unsigned long long sempty[kSSlots];
@@ -239,10 +242,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     S.abort_flag = 0;
     mbar_fence_init();
   }
-  if (tid < 16) S.str[tid >> 3][tid & 7][kZeroSlot] = 0.0;
+  if (tid < 24) S.str[tid >> 3][tid & 7][kZeroSlot] = 0.0;
   __syncthreads();
 
-  const int T0 = blockIdx.x, dT = gridDim.x;
+  const int T0 = a.run_off[blockIdx.x], T1 = a.run_off[blockIdx.x + 1];
   constexpr uint32_t kCsBytes = kConstStressFields * kTileOwned * 8u;
   constexpr size_t kBlk = (size_t)kConstFields * kTileOwned;  // doubles per constant block
 
@@ -269,8 +272,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     constexpr uint32_t kRecBytes = kRecInts * 4u;
     if (pw == 0 && lane == 0) {
       for (int r = 0; r < kRecRing; r++) {
-        const int t = T0 + r * dT;
-        if (t >= a.ntiles) break;
+        const int t = T0 + r;
+        if (t >= T1) break;
         mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
         bulk_g2s(S.rec[r], a.tile_rec + (size_t)t * kRecInts, kRecBytes, &S.rec_full[r]);
       }
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     int issued = 0;
     int nu = 0;  // stepu parts issued (counted by the bulk warp's lane 0)
     bool ok = true;
-    for (int t = T0; t < a.ntiles; t += dT) {
+    for (int t = T0; t < T1; t++) {
       const int r = issued % kRecRing;
       const int s = issued % kSSlots;
       const uint32_t use = (uint32_t)(issued / kSSlots);
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
           if (w && issued >= kSSlots) {
             // stepu part nu == issued - 2; its slot frees after stepu(nu - 1)
             w = mbar_wait(&S.uempty, (uint32_t)(nu - 1) & 1, a.err, 9) ? 1 : 0;
-            if (w) issue_stepu(a, S, T0 + (nu++) * dT);
+            if (w) issue_stepu(a, S, T0 + (nu++));
             if (w) w = mbar_wait(&S.sempty[s], (use - 1) & 1, a.err, 2) ? 1 : 0;
           }
           trace_stamp(a, issued, 4);
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
         else if (lane == 14)
           bulk_g2s(st.v, a.v_in + off, b8, &S.sfull[s]);
         if (lane == 0) {
-          if (issued == 0) issue_stepu(a, S, T0 + (nu++) * dT);
+          if (issued == 0) issue_stepu(a, S, T0 + (nu++));
           trace_stamp(a, issued, 6);
         }
       } else {
@@ -362,14 +365,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       stage_sync();  // handshake 2
       if (pw == 0) {
         if (lane == 0) trace_stamp(a, issued, 0);
-        const int tr = t + kRecRing * dT;
-        if (lane == 0 && tr < a.ntiles) {
+        const int tr = t + kRecRing;
+        if (lane == 0 && tr < T1) {
           mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
           bulk_g2s(S.rec[r], a.tile_rec + (size_t)tr * kRecInts, kRecBytes, &S.rec_full[r]);
         }
         if (a.prefetch > 0) {
-          const int tp = t + a.prefetch * dT;
-          if (tp < a.ntiles && lane < 15) {
+          const int tp = t + a.prefetch;
+          if (tp < T1 && lane < 15) {
             // what the stage load of a later tile copies: its constant block,
             // the owned ranges of the 12 stresses, u and v
             const int po = a.tile_meta[8 * tp], pc = a.tile_meta[8 * tp + 1];
@@ -390,7 +393,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
         // the stepu parts of the last tiles
         for (; nu < issued; nu++) {
           if (!mbar_wait(&S.uempty, (uint32_t)(nu - 1) & 1, a.err, 9)) break;
-          issue_stepu(a, S, T0 + nu * dT);
+          issue_stepu(a, S, T0 + nu);
         }
       }
       if (lane == 0 && nu > 0) mbar_wait(&S.ufull, (uint32_t)(nu - 1) & 1, a.err, 10);
@@ -405,8 +408,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       // records issued ahead and never consumed must land before exit too
       if (lane == 0) {
         for (int k = issued; k < issued + kRecRing; k++) {
-          const int t = T0 + k * dT;
-          if (t >= a.ntiles) break;
+          const int t = T0 + k;
+          if (t >= T1) break;
           mbar_wait(&S.rec_full[k % kRecRing], (uint32_t)(k / kRecRing) & 1, a.err, 7);
         }
       }
@@ -418,19 +421,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   // ========================= consumers ===================================
   // Per tile one block barrier: after stress, when the tile's str table is
   // complete.  Stepu then runs warp by warp and each warp goes straight on to
-  // the next tile's stress, so one warp's stepu overlaps the others' stress;
-  // str is double-buffered (stress of tile k+1 writes the other table, and
-  // every warp has finished stepu(k-1) before any passes the barrier of tile
-  // k).  The stepu slot is released by one arrival per warp.  A wait that ran
-  // out anywhere is OR-reduced at the barrier, so all consumers leave the
-  // loop together.
-  const int c = tid;  // compute-set index: owned c < 256, halo 256 + h
+  // the next tile's stress, so one warp's stepu overlaps the others' stress.
+  // Stepu of tile k reads the tables of tiles k and k-1 while stress of tile
+  // k+1 writes the third; the table it writes last held tile k-2, whose
+  // readers (stepu of k-2 and k-1) every warp has finished before any passes
+  // the barrier of tile k.  The stepu slot is released by one arrival per
+  // warp.  A wait that ran out anywhere is OR-reduced at the barrier, so all
+  // consumers leave the loop together.
+  const int c = tid;  // compute-set index: owned c < cnt, halo cnt + h
   const int lane = tid & 31;
   bool fail = false;
   int it = 0;
-  for (int t = T0; t < a.ntiles; t += dT, it++) {
+  for (int t = T0; t < T1; t++, it++) {
     const int s = it % kSSlots;
-    const int b = it & 1;
+    const int b = it % 3;
+    const int bp = (it + 2) % 3;  // the previous tile's table
     const bool have = mbar_wait(&S.sfull[s], (uint32_t)(it / kSSlots) & 1, a.err, 1);
     fail |= !have;
     if (tid == 0) trace_stamp(a, it, 1);
@@ -439,8 +444,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     // ---------------- phase 1: stress ------------------------------------
     // The owned thread keeps what stepu needs from the stress part (its
     // index word and velocity) so that the slot can be released after stress.
-    const bool own = c < kTileOwned;
-    const int h = c - kTileOwned;
     uint32_t m = 0;
     double uold = 0.0, vold = 0.0;
     int off = 0, cnt = 0;
@@ -448,7 +451,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       off = st.hdr[0];
       cnt = st.hdr[1];
       const int nh = st.hdr[2];
-      if (own ? c < cnt : h < nh) {
+      const bool own = c < cnt;
+      const int h = c - cnt;
+      if (own || h < nh) {
         uint32_t lc;
         if (own) {
           const unsigned long long ml = (unsigned long long)__double_as_longlong(st.cs[7][c]);
@@ -517,9 +522,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     fail |= !hu;
     if (hu && c < cnt && !((m >> 30) & kSkipU)) {
       const USlot &us = S.us;
-      const double(&str)[8][kZeroSlot + 2] = S.str[b];
-      const int lnw = m & kLnbMask, lsw = (m >> kLnbBits) & kLnbMask;
-      const int lsse = (m >> (2 * kLnbBits)) & kLnbMask;
+      const double(&str)[8][kStrRow] = S.str[b];
+      // a neighbour's str: own table, or the previous tile's (kStrPrev)
+      const uint32_t vnw = m & kLnbMask, vsw = (m >> kLnbBits) & kLnbMask;
+      const uint32_t vsse = (m >> (2 * kLnbBits)) & kLnbMask;
+      const double(&tnw)[8][kStrRow] = (vnw & kStrPrev) ? S.str[bp] : S.str[b];
+      const double(&tsw)[8][kStrRow] = (vsw & kStrPrev) ? S.str[bp] : S.str[b];
+      const double(&tsse)[8][kStrRow] = (vsse & kStrPrev) ? S.str[bp] : S.str[b];
+      const int lnw = vnw & (kStrPrev - 1), lsw = vsw & (kStrPrev - 1);
+      const int lsse = vsse & (kStrPrev - 1);
       StepuIn in;
       in.uold = uold;
       in.vold = vold;
@@ -537,13 +548,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       in.uinit = us.cu[11][c];
       in.vinit = us.cu[12][c];
       in.s1 = str[0][c];
-      in.s2nw = str[1][lnw];
-      in.s3sse = str[2][lsse];
-      in.s4sw = str[3][lsw];
+      in.s2nw = tnw[1][lnw];
+      in.s3sse = tsse[2][lsse];
+      in.s4sw = tsw[3][lsw];
       in.s5 = str[4][c];
-      in.s6sse = str[5][lsse];
-      in.s7nw = str[6][lnw];
-      in.s8sw = str[7][lsw];
+      in.s6sse = tsse[5][lsse];
+      in.s7nw = tnw[6][lnw];
+      in.s8sw = tsw[7][lsw];
       const StepuOut o = stepu_point(in, p);
       a.u_out[off + c] = o.u;
       a.v_out[off + c] = o.v;
@@ -615,9 +626,9 @@ int tma_prepare(int device) {
   return e == cudaSuccess ? 0 : (int)e;
 }
 
-void launch_tma(const TmaArgs &a, const Params &p, bool last, int nctas, cudaStream_t st) {
-  if (a.ntiles <= 0) return;
-  const int grid = a.ntiles < nctas ? a.ntiles : nctas;
+void launch_tma(const TmaArgs &a, const Params &p, bool last, cudaStream_t st) {
+  if (a.ntiles <= 0 || a.nruns <= 0) return;
+  const int grid = a.nruns;
   const bool std = std_params(p);
   if (last && std)
     k_tma<true, true><<<grid, kThreads, smem_bytes(), st>>>(a, p);

@@ -1,8 +1,9 @@
 // evp_plan_check.cpp -- host-side verification of a tile plan.
 //
 // The kernels gather through indices that the planner derives from the
-// neighbour vectors: slot positions, forward-halo lists, velocity extras and
-// 10-bit local indices packed three to a word.  A wrong one would read the
+// neighbour vectors: slot positions, runs of tiles, forward-halo lists,
+// velocity extras and 10-bit local indices packed three to a word (a str
+// index may point into the previous tile of the same run).  A wrong one would read the
 // wrong point (or outside a shared-memory array) without any fault to show
 // it.  This check decodes every such index and compares it with what the
 // neighbour vectors say it must be, so a plan is known good before any
@@ -52,6 +53,8 @@ long long verify_tile_plan(const TilePlan &P, const int32_t *const nb0[6], int m
          P.point_of_slot.size());
   for (const auto *v : {&P.tile_off, &P.tile_cnt, &P.halo_off, &P.halo_cnt, &P.uvx_off, &P.uvx_cnt})
     if (v->size() != (size_t)T) note(bad, first, "a per-tile array has %zu entries", v->size());
+  if (P.nruns < 0 || P.run_off.size() != (size_t)P.nruns + 1)
+    note(bad, first, "%d runs with %zu run offsets", P.nruns, P.run_off.size());
   for (int r = 0; r < 6; r++)
     if (nbs[r]->size() != (size_t)S) note(bad, first, "neighbour slots %d: %zu entries", r, nbs[r]->size());
   if (P.lnb.size() != (size_t)S || P.lcor.size() != (size_t)S)
@@ -104,6 +107,18 @@ long long verify_tile_plan(const TilePlan &P, const int32_t *const nb0[6], int m
   for (int s = 0; s < S; s++)
     if (tile_of[s] < 0 && P.point_of_slot[s] >= 0)
       note(bad, first, "point %d (slot %d) is in no tile", P.point_of_slot[s], s);
+  // runs: consecutive non-empty tile ranges that cover every tile once
+  std::vector<char> first_of_run((size_t)T, 0);
+  if (P.run_off.front() != 0 || P.run_off.back() != T)
+    note(bad, first, "runs cover tiles [%d, %d), not [0, %d)", P.run_off.front(), P.run_off.back(),
+         T);
+  for (int r = 0; r < P.nruns; r++) {
+    if (P.run_off[r + 1] <= P.run_off[r]) {
+      note(bad, first, "run %d is [%d, %d)", r, P.run_off[r], P.run_off[r + 1]);
+      continue;
+    }
+    if (P.run_off[r] >= 0 && P.run_off[r] < T) first_of_run[P.run_off[r]] = 1;
+  }
   if (bad) return bad;
 
   auto to_slot = [&](int n) { return n < na ? P.slot_of_point[n] : S + (n - na); };
@@ -118,17 +133,27 @@ long long verify_tile_plan(const TilePlan &P, const int32_t *const nb0[6], int m
     }
   }
 
-  // per tile: forward halo, velocity extras and every packed local index
+  // per tile: forward halo, velocity extras and every packed local index.
+  // ppos: str-table position of a slot in the previous tile's compute set
+  // (owned: slot offset; halo h: that tile's count + h), -1 elsewhere.
   std::vector<int32_t> hpos((size_t)S, -1), xpos((size_t)nuv, -1);
+  std::vector<int32_t> ppos((size_t)S, -1), pslots;
   std::vector<char> hused((size_t)kTileHalo), xused((size_t)kTileUvx);
   for (int t = 0; t < T; t++) {
     if (!tile_ok[t]) continue;
     const int off = P.tile_off[t], cnt = P.tile_cnt[t];
     const int ho = P.halo_off[t], hc = P.halo_cnt[t], xo = P.uvx_off[t], xc = P.uvx_cnt[t];
+    // the previous tile's table is alive only inside a run
+    if (first_of_run[t]) {
+      for (int sl : pslots) ppos[sl] = -1;
+      pslots.clear();
+    }
     if (hc < 0 || hc > kTileHalo || ho < 0 || (size_t)ho + hc > nh_all) {
       note(bad, first, "tile %d halo list [%d, +%d) is out of bounds", t, ho, hc);
       continue;
     }
+    if (cnt + hc > max_tile || cnt + hc > kTileCompute)
+      note(bad, first, "tile %d computes %d + %d points (limit %d)", t, cnt, hc, max_tile);
     if (xc < 0 || xc > kTileUvx || xo < 0 || (size_t)xo + xc > nx_all) {
       note(bad, first, "tile %d extra list [%d, +%d) is out of bounds", t, xo, xc);
       continue;
@@ -139,6 +164,8 @@ long long verify_tile_plan(const TilePlan &P, const int32_t *const nb0[6], int m
         note(bad, first, "tile %d halo %d: slot %d is no list point", t, h, s);
       else if (tile_of[s] == t)
         note(bad, first, "tile %d halo %d: slot %d is the tile's own", t, h, s);
+      else if (ppos[s] >= 0)
+        note(bad, first, "tile %d halo %d: slot %d is in the previous tile's table", t, h, s);
       else if (hpos[s] >= 0)
         note(bad, first, "tile %d halo repeats slot %d", t, s);
       else
@@ -176,8 +203,10 @@ long long verify_tile_plan(const TilePlan &P, const int32_t *const nb0[6], int m
           const int sl = P.slot_of_point[n];
           if (tile_of[sl] == t) {
             want = sl - off;
+          } else if (ppos[sl] >= 0) {
+            want = (int)kStrPrev | ppos[sl];
           } else if (hpos[sl] >= 0) {
-            want = kTileOwned + hpos[sl];
+            want = cnt + hpos[sl];
             hused[hpos[sl]] = 1;
           } else {
             want = -1;
@@ -215,9 +244,20 @@ long long verify_tile_plan(const TilePlan &P, const int32_t *const nb0[6], int m
     }
     for (int x = 0; x < xc; x++)
       if (!xused[x]) note(bad, first, "tile %d extra %d is read by no point", t, x);
+    // this tile's compute set becomes the previous table
+    for (int sl : pslots) ppos[sl] = -1;
+    pslots.clear();
+    for (int s = off; s < off + cnt; s++) {
+      ppos[s] = s - off;
+      pslots.push_back(s);
+    }
     for (int h = 0; h < hc; h++) {
       const int s = P.halo_idx[ho + h];
-      if (s >= 0 && s < S) hpos[s] = -1;
+      if (s >= 0 && s < S) {
+        hpos[s] = -1;
+        ppos[s] = cnt + h;
+        pslots.push_back(s);
+      }
     }
     for (int x = 0; x < xc; x++) {
       const int s = P.uvx_idx[xo + x];

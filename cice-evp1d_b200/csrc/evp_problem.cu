@@ -63,6 +63,7 @@ void layout(DeviceProblem *d, Carve &c, size_t nhalo_total, size_t nuvx_total) {
   c.take(&d->tile_meta, 8 * T);
   c.take(&d->tile_rec, (size_t)kRecInts * T);
   c.take(&d->cblk, (size_t)kConstFields * kConstTileSlots * T);
+  c.take(&d->run_off, (size_t)d->nruns + 1);
   c.take(&d->tile_off, T);
   c.take(&d->tile_cnt, T);
   c.take(&d->halo_off, T);
@@ -98,6 +99,7 @@ int problem_create(DeviceProblem *d, int device, const TilePlan &plan,
   d->nhs = plan.nhalo_slots;
   d->nuv = plan.nslots + plan.nhalo_slots;
   d->ntiles = plan.ntiles;
+  d->nruns = plan.nruns;
   d->from_coords = plan.from_coords;
   CUDA_TRY(cudaSetDevice(device));
   CUDA_TRY(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
@@ -119,6 +121,7 @@ int problem_create(DeviceProblem *d, int device, const TilePlan &plan,
   }
   const size_t T = (size_t)d->ntiles * sizeof(int32_t);
   const size_t S4 = (size_t)d->nslots * sizeof(int32_t);
+  TRY(h2d(d->run_off, plan.run_off.data(), plan.run_off.size() * sizeof(int32_t), st));
   TRY(h2d(d->tile_off, plan.tile_off.data(), T, st));
   TRY(h2d(d->tile_cnt, plan.tile_cnt.data(), T, st));
   TRY(h2d(d->halo_off, plan.halo_off.data(), T, st));
@@ -405,6 +408,8 @@ FusedArgs problem_fused_args(const DeviceProblem &d, int from) {
   FusedArgs a;
   const int to = 1 - from;
   a.ntiles = d.ntiles;
+  a.nruns = d.nruns;
+  a.run_off = d.run_off;
   a.tile_off = d.tile_off;
   a.tile_cnt = d.tile_cnt;
   a.halo_off = d.halo_off;
@@ -454,6 +459,8 @@ TmaArgs problem_tma_args(const DeviceProblem &d, int from) {
   TmaArgs a;
   const int to = 1 - from;
   a.ntiles = d.ntiles;
+  a.nruns = d.nruns;
+  a.run_off = d.run_off;
   a.tile_off = d.tile_off;
   a.tile_cnt = d.tile_cnt;
   a.halo_off = d.halo_off;

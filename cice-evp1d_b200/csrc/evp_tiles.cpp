@@ -6,11 +6,20 @@
 //   sse = (i,j+1) (integration/ice_dyn_evp1d.F90:766-772).  Each connected
 //   piece of the list gets its own origin.  A graph that contradicts itself
 //   (two coordinates for one point, or two points on one coordinate) has no
-//   grid layout, and the plan then tiles consecutive list points instead.
-// Step 2: tiles.  Points are grouped by (piece, j / kTileH, i / kTileW), tiles
-//   ordered row by row, points row by row inside a tile.
-// Step 3: forward halo.  A tile whose halo would exceed kTileHalo points is
-//   split in halves until it fits (possible only for irregular graphs).
+//   grid layout, and the points then keep their list order.
+// Step 2: order.  Each piece is cut into strips of strip_w columns; a strip's
+//   points are taken row by row from the top row down, each row right to
+//   left.  stepu's neighbours nw, sw, sse lie at +i or +j, so every one of
+//   them inside the strip comes at most strip_w + 1 places EARLIER in this
+//   order: in the same tile, or in the tile before it.  Only the strip's
+//   right edge (about one point per row) and the top of a run need their
+//   stress recomputed as a forward halo.
+// Step 3: runs and tiles.  The order is cut into runs of at most K tiles, one
+//   run per CTA, K as small as the CTA count allows.  Within a run each tile
+//   takes the longest prefix of the remaining points whose compute set
+//   (owned points plus the forward-halo points that neither this tile nor
+//   the run's previous tile holds) fits max_tile threads, kTileHalo halo
+//   points and kTileUvx extra velocities.
 #include "evp_tiles.h"
 
 #include <algorithm>
@@ -24,29 +33,6 @@ namespace {
 
 const int kDI[6] = {-1, -1, 0, +1, +1, 0};  // ee ne se nw sw sse
 const int kDJ[6] = {0, -1, -1, 0, +1, +1};
-
-inline int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
-
-// Position of (x, y) along the Hilbert curve filling the n x n square (n a
-// power of two), by the standard rotate-and-reflect walk over the quadrant
-// bits (the published xy-to-d conversion).
-uint64_t hilbert_index(uint32_t n, uint32_t x, uint32_t y) {
-  uint64_t d = 0;
-  for (uint32_t s = n / 2; s > 0; s /= 2) {
-    const uint32_t rx = (x & s) ? 1u : 0u, ry = (y & s) ? 1u : 0u;
-    d += (uint64_t)s * (uint64_t)s * ((3u * rx) ^ ry);
-    if (ry == 0) {
-      if (rx == 1) {
-        x = s - 1 - x;
-        y = s - 1 - y;
-      }
-      const uint32_t t = x;
-      x = y;
-      y = t;
-    }
-  }
-  return d;
-}
 
 bool reconstruct_coords(int na, const int32_t *const nb0[6],
                         std::vector<int32_t> &ci, std::vector<int32_t> &cj,
@@ -97,22 +83,201 @@ bool reconstruct_coords(int na, const int32_t *const nb0[6],
   return true;
 }
 
+// The points of every piece in strips (step 2), pieces in a canonical order
+// that does not depend on the list order: larger first, then by extent, then
+// by the position of the piece's first point in its own strip order.
+std::vector<int32_t> strip_order(int na, std::vector<int32_t> &ci, std::vector<int32_t> &cj,
+                                 const std::vector<int32_t> &comp, int strip_w) {
+  int nc = 0;
+  for (int p = 0; p < na; p++) nc = comp[p] + 1 > nc ? comp[p] + 1 : nc;
+  std::vector<int32_t> mi((size_t)nc, INT_MAX), mj((size_t)nc, INT_MAX);
+  for (int p = 0; p < na; p++) {
+    mi[comp[p]] = std::min(mi[comp[p]], ci[p]);
+    mj[comp[p]] = std::min(mj[comp[p]], cj[p]);
+  }
+  for (int p = 0; p < na; p++) {
+    ci[p] -= mi[comp[p]];
+    cj[p] -= mj[comp[p]];
+  }
+  std::vector<int32_t> pn((size_t)nc, 0), pw((size_t)nc, 0), ph((size_t)nc, 0);
+  for (int p = 0; p < na; p++) {
+    pn[comp[p]]++;
+    pw[comp[p]] = std::max(pw[comp[p]], ci[p] + 1);
+    ph[comp[p]] = std::max(ph[comp[p]], cj[p] + 1);
+  }
+  // position in the strip order of a piece: strip, then rows top down, then
+  // columns right to left
+  auto key = [&](int p) -> long long {
+    const long long strip = ci[p] / strip_w;
+    return (strip * (long long)(ph[comp[p]] + 1) + (ph[comp[p]] - 1 - cj[p])) * (long long)(strip_w + 1) +
+           (strip_w - 1 - ci[p] % strip_w);
+  };
+  std::vector<long long> pfirst((size_t)nc, LLONG_MAX);
+  for (int p = 0; p < na; p++) pfirst[comp[p]] = std::min(pfirst[comp[p]], key(p));
+  std::vector<int32_t> order((size_t)na);
+  for (int p = 0; p < na; p++) order[p] = p;
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    const int A = comp[a], B = comp[b];
+    if (A != B) {
+      if (pn[A] != pn[B]) return pn[A] > pn[B];
+      if (pw[A] != pw[B]) return pw[A] < pw[B];
+      if (ph[A] != ph[B]) return ph[A] < ph[B];
+      if (pfirst[A] != pfirst[B]) return pfirst[A] < pfirst[B];
+      return A < B;
+    }
+    return key(a) < key(b);
+  });
+  return order;
+}
+
+// Incremental bookkeeping of one tile under construction (step 3): points
+// join in order, and the forward halo and the extra velocities are kept
+// counted with reference counts, so that the longest fitting prefix is found
+// in one pass.
+class TileBuilder {
+ public:
+  TileBuilder(int na, int navel, const int32_t *const nb0[6])
+      : na_(na), nb_(nb0), owned_(navel, 0), prev_(navel, 0), href_(navel, 0),
+        xref_(navel, 0) {}
+
+  // Start a tile; `prev` = the compute set of the run's previous tile
+  // (empty for the first tile of a run).
+  void begin(const std::vector<int32_t> &prev) {
+    clear();
+    for (int q : prev) prev_[q] = 1;
+    prev_list_ = prev;
+  }
+
+  void add(int p) {
+    if (in_halo(p)) {  // p was a halo point: drop what it asked for
+      nh_--;
+      xdec(p);
+      for (int r = 0; r < 3; r++) xdec(nb_[r][p]);
+    }
+    if (xref_[p] > 0) nx_--;  // p no longer an extra velocity
+    owned_[p] = 1;
+    touch(p);
+    members_.push_back(p);
+    for (int r = 0; r < 3; r++) xinc(nb_[r][p]);
+    for (int r = 3; r < 6; r++) {
+      const int q = nb_[r][p];
+      if (q >= na_) continue;
+      touch(q);
+      if (++href_[q] == 1 && !owned_[q] && !prev_[q]) {
+        nh_++;
+        xinc(q);
+        for (int r2 = 0; r2 < 3; r2++) xinc(nb_[r2][q]);
+      }
+    }
+  }
+
+  int owned() const { return (int)members_.size(); }
+  int halo() const { return nh_; }
+  int extras() const { return nx_; }
+
+  // The forward-halo points, in the order the owned points first reach them.
+  std::vector<int32_t> halo_list() const {
+    std::vector<int32_t> h;
+    std::vector<int32_t> seen;
+    for (int p : members_)
+      for (int r = 3; r < 6; r++) {
+        const int q = nb_[r][p];
+        if (q < na_ && in_halo(q) && std::find(seen.begin(), seen.end(), q) == seen.end()) {
+          seen.push_back(q);
+          h.push_back(q);
+        }
+      }
+    return h;
+  }
+
+  void clear() {
+    for (int q : touched_) owned_[q] = href_[q] = xref_[q] = 0;
+    for (int q : prev_list_) prev_[q] = 0;
+    touched_.clear();
+    prev_list_.clear();
+    members_.clear();
+    nh_ = nx_ = 0;
+  }
+
+ private:
+  bool in_halo(int q) const { return q < na_ && href_[q] > 0 && !owned_[q] && !prev_[q]; }
+  void touch(int q) { touched_.push_back(q); }
+  void xinc(int q) {
+    touch(q);
+    if (++xref_[q] == 1 && !owned_[q]) nx_++;
+  }
+  void xdec(int q) {
+    if (--xref_[q] == 0 && !owned_[q]) nx_--;
+  }
+
+  int na_;
+  const int32_t *const *nb_;
+  std::vector<int32_t> owned_, prev_, href_, xref_;
+  std::vector<int32_t> touched_, prev_list_, members_;
+  int nh_ = 0, nx_ = 0;
+};
+
+struct Tiling {
+  std::vector<std::vector<int32_t>> tiles;  // owned points of each tile
+  std::vector<int32_t> run_off;
+};
+
+// Tiles of order[k0, k1) in runs of at most `per_run` tiles; a run never
+// holds a previous-tile reference in its first tile.  per_run <= 0: one run.
+Tiling make_tiles(TileBuilder &tb, const std::vector<int32_t> &order, int max_tile, int per_run) {
+  Tiling T;
+  T.run_off.push_back(0);
+  const int n = (int)order.size();
+  std::vector<int32_t> prev;
+  int in_run = 0;
+  for (int k = 0; k < n;) {
+    if (per_run > 0 && in_run == per_run) {
+      T.run_off.push_back((int)T.tiles.size());
+      in_run = 0;
+      prev.clear();
+    }
+    tb.begin(prev);
+    int best = 1;
+    // the counts are not monotone in the prefix length (a later point can
+    // absorb a halo point), so every length up to the cap is tried
+    for (int len = 1; len <= max_tile && k + len <= n; len++) {
+      tb.add(order[k + len - 1]);
+      if (len + tb.halo() <= max_tile && tb.halo() <= kTileHalo && tb.extras() <= kTileUvx)
+        best = len;
+    }
+    // the chosen prefix again, for its halo list
+    tb.begin(prev);
+    for (int q = 0; q < best; q++) tb.add(order[k + q]);
+    std::vector<int32_t> members(order.begin() + k, order.begin() + k + best);
+    prev = members;
+    for (int q : tb.halo_list()) prev.push_back(q);
+    tb.clear();
+    T.tiles.push_back(std::move(members));
+    in_run++;
+    k += best;
+  }
+  T.run_off.push_back((int)T.tiles.size());
+  return T;
+}
+
 }  // namespace
 
 void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
                      const int32_t *coords_i, const int32_t *coords_j,
-                     TilePlan *plan, int max_tile) {
-  const int tmax = max_tile < 1 ? 1 : (max_tile > kTileOwned ? kTileOwned : max_tile);
+                     TilePlan *plan, int max_tile, int nruns, int strip_w) {
+  const int tmax = max_tile < 1 ? 1 : (max_tile > kTileCompute ? kTileCompute : max_tile);
+  const int want_runs = nruns < 1 ? 1 : nruns;
+  const int w = strip_w < 1 ? 1 : strip_w;
   TilePlan &P = *plan;
   P = TilePlan();
   P.na = na;
   P.navel = navel;
   P.nhalo_slots = navel - na;
+  P.run_off.assign(1, 0);
   if (na == 0) return;
 
-  // ---- step 1 + 2: candidate groups --------------------------------------
-  std::vector<std::vector<int32_t>> groups;
-  std::vector<int32_t> ci, cj, comp;
+  // ---- steps 1 + 2: the order ----------------------------------------------
+  std::vector<int32_t> ci, cj, comp, order;
   bool have = false;
   if (coords_i && coords_j) {
     ci.assign(coords_i, coords_i + na);
@@ -124,155 +289,24 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
   }
   P.from_coords = have;
   if (have) {
-    // origin of each piece at its bounding-box corner, so that the tiles do
-    // not depend on where the walk started (i.e. on the list order)
-    int nc = 0;
-    for (int p = 0; p < na; p++) nc = comp[p] + 1 > nc ? comp[p] + 1 : nc;
-    std::vector<int32_t> mi((size_t)nc, INT_MAX), mj((size_t)nc, INT_MAX);
-    for (int p = 0; p < na; p++) {
-      mi[comp[p]] = ci[p] < mi[comp[p]] ? ci[p] : mi[comp[p]];
-      mj[comp[p]] = cj[p] < mj[comp[p]] ? cj[p] : mj[comp[p]];
-    }
-    for (int p = 0; p < na; p++) {
-      ci[p] -= mi[comp[p]];
-      cj[p] -= mj[comp[p]];
-    }
-    // pieces in a canonical order (by their position in the grid walk's
-    // coordinates is not canonical, so by size and extent), points of a piece
-    // along a Hilbert curve over its coordinates, then consecutive runs of
-    // tmax points: compact, full tiles.  A run may span two pieces;
-    // pieces never share neighbours, so that only merges small floes.
-    std::vector<int32_t> pn((size_t)nc, 0), pw((size_t)nc, 0), ph((size_t)nc, 0);
-    for (int p = 0; p < na; p++) {
-      pn[comp[p]]++;
-      pw[comp[p]] = ci[p] + 1 > pw[comp[p]] ? ci[p] + 1 : pw[comp[p]];
-      ph[comp[p]] = cj[p] + 1 > ph[comp[p]] ? cj[p] + 1 : ph[comp[p]];
-    }
-    std::vector<uint64_t> hkey((size_t)na);
-    for (int p = 0; p < na; p++) {
-      uint32_t n = 1;
-      const int32_t ext = pw[comp[p]] > ph[comp[p]] ? pw[comp[p]] : ph[comp[p]];
-      while ((int64_t)n < ext) n *= 2;
-      hkey[p] = hilbert_index(n, (uint32_t)ci[p], (uint32_t)cj[p]);
-    }
-    // canonical piece order: larger first, then by extent and the first
-    // point's Hilbert position -- none of which depends on the list order
-    std::vector<uint64_t> pfirst((size_t)nc, UINT64_MAX);
-    for (int p = 0; p < na; p++) pfirst[comp[p]] = hkey[p] < pfirst[comp[p]] ? hkey[p] : pfirst[comp[p]];
-    std::vector<int32_t> order((size_t)na);
-    for (int p = 0; p < na; p++) order[p] = p;
-    std::sort(order.begin(), order.end(), [&](int a, int b) {
-      const int A = comp[a], B = comp[b];
-      if (A != B) {
-        if (pn[A] != pn[B]) return pn[A] > pn[B];
-        if (pw[A] != pw[B]) return pw[A] < pw[B];
-        if (ph[A] != ph[B]) return ph[A] < ph[B];
-        if (pfirst[A] != pfirst[B]) return pfirst[A] < pfirst[B];
-        return A < B;
-      }
-      return hkey[a] < hkey[b];
-    });
-    // each tile takes the longest run (up to tmax points) whose halo
-    // and velocity extras fit, found by bisection on the run length
-    std::vector<int32_t> m1((size_t)navel, -1), m2((size_t)navel, -1), m3((size_t)navel, -1);
-    int st = 0;
-    auto fits = [&](int k, int len) {
-      st++;
-      for (int q = k; q < k + len; q++) m1[order[q]] = st;
-      int nh = 0, nx = 0;
-      std::vector<int32_t> hl;
-      for (int q = k; q < k + len; q++)
-        for (int r = 3; r < 6; r++) {
-          const int n = nb0[r][order[q]];
-          if (n < na && m1[n] != st && m2[n] != st) {
-            m2[n] = st;
-            hl.push_back(n);
-            if (++nh > kTileHalo) return false;
-          }
-        }
-      auto add_x = [&](int n) {
-        if (m1[n] != st && m3[n] != st) {
-          m3[n] = st;
-          nx++;
-        }
-      };
-      for (int n : hl) add_x(n);
-      for (int q = k; q < k + len; q++)
-        for (int r = 0; r < 3; r++) add_x(nb0[r][order[q]]);
-      for (int n : hl)
-        for (int r = 0; r < 3; r++) add_x(nb0[r][n]);
-      return nx <= kTileUvx;
-    };
-    for (int k = 0; k < na;) {
-      int len = tmax < na - k ? tmax : na - k;
-      if (!fits(k, len)) {
-        int lo = 1, hi = len - 1;  // fits(k, 1) holds: a point reaches 3 + 6 + 9 others
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) / 2;
-          if (fits(k, mid)) lo = mid; else hi = mid - 1;
-        }
-        len = lo;
-      }
-      groups.emplace_back(order.begin() + k, order.begin() + k + len);
-      k += len;
-    }
+    order = strip_order(na, ci, cj, comp, w);
   } else {
-    for (int k = 0; k < na; k += tmax) {
-      std::vector<int32_t> g;
-      for (int p = k; p < na && p < k + tmax; p++) g.push_back(p);
-      groups.push_back(std::move(g));
-    }
+    order.resize((size_t)na);
+    for (int p = 0; p < na; p++) order[p] = p;
   }
 
-  // ---- step 3: split groups whose halo or velocity set is too large ------
-  // halo H = list points outside the group reached through nw/sw/sse;
-  // extras X = ({H} + ee/ne/se of group and H) minus the group, where the
-  // reference's halo slots (>= na) count as points too.
-  std::vector<int32_t> mark((size_t)navel, -1), hmark((size_t)navel, -1),
-      xmark((size_t)navel, -1);
-  int stamp = 0;
-  std::vector<std::vector<int32_t>> tiles;
-  std::vector<std::vector<int32_t>> stack;
-  std::vector<int32_t> hl;
-  for (auto &g0 : groups) {
-    stack.push_back(std::move(g0));
-    while (!stack.empty()) {
-      std::vector<int32_t> g = std::move(stack.back());
-      stack.pop_back();
-      stamp++;
-      for (int p : g) mark[p] = stamp;
-      int nh = 0, nx = 0;
-      hl.clear();
-      for (int p : g)
-        for (int r = 3; r < 6; r++) {
-          const int n = nb0[r][p];
-          if (n < na && mark[n] != stamp && hmark[n] != stamp) {
-            hmark[n] = stamp;
-            hl.push_back(n);
-            nh++;
-          }
-        }
-      auto add_x = [&](int n) {
-        if (mark[n] != stamp && xmark[n] != stamp) {
-          xmark[n] = stamp;
-          nx++;
-        }
-      };
-      for (int q : hl) add_x(q);
-      for (int p : g)
-        for (int r = 0; r < 3; r++) add_x(nb0[r][p]);
-      for (int q : hl)
-        for (int r = 0; r < 3; r++) add_x(nb0[r][q]);
-      if ((int)g.size() <= tmax && nh <= kTileHalo && nx <= kTileUvx) {
-        tiles.push_back(std::move(g));
-      } else {
-        const size_t half = g.size() / 2;
-        std::vector<int32_t> a(g.begin(), g.begin() + half), b(g.begin() + half, g.end());
-        stack.push_back(std::move(b));
-        stack.push_back(std::move(a));
-      }
-    }
+  // ---- step 3: runs of at most K tiles, K as small as the CTAs allow -------
+  TileBuilder tb(na, navel, nb0);
+  const Tiling whole = make_tiles(tb, order, tmax, 0);
+  int K = ((int)whole.tiles.size() + want_runs - 1) / want_runs;
+  Tiling T;
+  for (;; K++) {
+    T = make_tiles(tb, order, tmax, K);
+    if ((int)T.run_off.size() - 1 <= want_runs) break;
   }
+  std::vector<std::vector<int32_t>> &tiles = T.tiles;
+  P.nruns = (int)T.run_off.size() - 1;
+  P.run_off = T.run_off;
 
   // ---- slots ---------------------------------------------------------------
   P.ntiles = (int)tiles.size();
@@ -314,16 +348,26 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
   P.halo_cnt.resize(P.ntiles);
   P.uvx_off.resize(P.ntiles);
   P.uvx_cnt.resize(P.ntiles);
-  // hpos/htile: forward-halo position of a list point in the current tile;
-  // xpos/xtile: velocity-extra position of any u/v point (list or halo slot)
-  std::vector<int32_t> hpos((size_t)na, -1), htile((size_t)na, -1);
+  std::vector<char> first_of_run((size_t)P.ntiles, 0);
+  for (int r = 0; r < P.nruns; r++)
+    if (P.run_off[r] < P.ntiles) first_of_run[P.run_off[r]] = 1;
+  // cpos/ctile: str-table position of a list point in tile ctile's compute
+  // set (owned: its slot offset; halo h: tile_cnt + h), for the current and
+  // the previous tile; xpos/xtile: velocity-extra position of any u/v point
+  std::vector<int32_t> cpos((size_t)na, -1), ctile((size_t)na, -1);
+  std::vector<int32_t> ppos((size_t)na, -1), ptile((size_t)na, -1);
   std::vector<int32_t> xpos((size_t)navel, -1), xtile((size_t)navel, -1);
   for (int t = 0; t < P.ntiles; t++) {
     P.halo_off[t] = (int)P.halo_idx.size();
     P.uvx_off[t] = (int)P.uvx_idx.size();
     int nh = 0, nx = 0;
     const int own = P.tile_cnt[t];
+    const bool has_prev = !first_of_run[t];
     std::vector<int32_t> &members = tiles[t];
+    for (int k = 0; k < own; k++) {
+      ctile[members[k]] = t;
+      cpos[members[k]] = k;
+    }
     // stepu's str neighbours and the forward halo
     for (int k = 0; k < own; k++) {
       const int p = members[k];
@@ -333,15 +377,15 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
         uint32_t loc;
         if (n >= na) {
           loc = kZeroSlot;
-        } else if (tile_of[n] == t) {
-          loc = (uint32_t)(P.slot_of_point[n] - P.tile_off[t]);
+        } else if (ctile[n] == t) {
+          loc = (uint32_t)cpos[n];
+        } else if (has_prev && ptile[n] == t - 1) {
+          loc = kStrPrev | (uint32_t)ppos[n];
         } else {
-          if (htile[n] != t) {  // first time this tile reaches n
-            htile[n] = t;
-            hpos[n] = nh++;
-            P.halo_idx.push_back(P.slot_of_point[n]);
-          }
-          loc = (uint32_t)(kTileOwned + hpos[n]);
+          ctile[n] = t;  // first time this tile reaches n: a halo point
+          cpos[n] = own + nh++;
+          P.halo_idx.push_back(P.slot_of_point[n]);
+          loc = (uint32_t)cpos[n];
         }
         packed |= loc << ((r - 3) * kLnbBits);
       }
@@ -372,6 +416,16 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
     }
     P.halo_cnt[t] = nh;
     P.uvx_cnt[t] = nx;
+    // this tile's compute set is the next tile's previous table
+    for (int k = 0; k < own; k++) {
+      ptile[members[k]] = t;
+      ppos[members[k]] = k;
+    }
+    for (int h = 0; h < nh; h++) {
+      const int q = P.point_of_slot[P.halo_idx[P.halo_off[t] + h]];
+      ptile[q] = t;
+      ppos[q] = own + h;
+    }
   }
 }
 

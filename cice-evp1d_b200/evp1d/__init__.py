@@ -175,7 +175,7 @@ def plan_stats(na: int, navel: int, idx: dict) -> dict:
     check(L.evp1d_plan_stats(int(na), int(navel), *[a.ctypes.data_as(_I) for a in arrs], st),
           "evp1d_plan_stats")
     return dict(tiles=st[0], slots=st[1], halo=st[2], from_coords=bool(st[3]),
-                max_halo=st[4], max_tile=st[5], max_extras=st[6])
+                max_halo=st[4], max_tile=st[5], max_extras=st[6], max_run_tiles=st[7])
 
 
 class FieldSet:

@@ -270,7 +270,8 @@ int evp1d_dyn_finalize(evp1d_dyn_t *handle);
 /* Number of 1D list points (nActive) and slots (navel) of a 2D handle. */
 int evp1d_dyn_sizes(evp1d_dyn_t *handle, int *na, int *navel);
 
-/* Largest tile, in list points, of the tile plans of handles created after
+/* Largest tile compute set (owned points plus recomputed forward-halo
+ * points; one kernel thread each) of the tile plans of handles created after
  * the call (evp1d_init, evp1d_init_batched, and evp1d_plan_stats); 32..256,
  * default 256.  Process-wide; handles that exist keep their plan.  No
  * counterpart in the reference: a dimension for the autotuner
@@ -322,7 +323,9 @@ int evp1d_exchange_buffers(evp1d_t *handle, double **send, double **recv);
  * coordinates rebuilt from the neighbour vectors (0: consecutive list points),
  * [4] largest halo of one tile, [5] largest tile, [6] largest number of
  * extra velocity points (read by the stencil, owned by no tile point) of one
- * tile.
+ * tile, [7] largest number of tiles in one run (the tiles one CTA of the
+ * subcycle kernel works through; the plan is made for 148 CTAs, a B200's SM
+ * count).
  * -------------------------------------------------------------------------- */
 int evp1d_plan_stats(int na, int navel, const int32_t *ee, const int32_t *ne,
                      const int32_t *se, const int32_t *nw, const int32_t *sw,

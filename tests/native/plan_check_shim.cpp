@@ -43,6 +43,35 @@ bool plant(evp::TilePlan &P, int kind) {
     case 11: P.point_of_slot[off] = -1; return true;                // point lost
     case 12: P.halo_cnt[t] -= 1; return true;                       // halo entry missing
     case 13: P.uvx_cnt[t] -= 1; return true;                        // extra missing
+    case 14: {  // a previous-table str index in the first tile of a run
+      if (P.nruns < 2) return false;
+      const int f = P.run_off[1];
+      P.lnb[P.tile_off[f]] = (P.lnb[P.tile_off[f]] & ~evp::kLnbMask) | evp::kStrPrev;
+      return true;
+    }
+    case 15: {  // an empty run
+      if (P.nruns < 2) return false;
+      P.run_off[1] = P.run_off[0];
+      return true;
+    }
+    case 16: {  // a previous-table index to a point the previous tile lacks
+      for (int u = 1; u < P.ntiles; u++) {
+        bool first_of_run = false;
+        for (int r = 0; r <= P.nruns; r++) first_of_run |= P.run_off[r] == u;
+        if (first_of_run) continue;
+        for (int s = P.tile_off[u]; s < P.tile_off[u] + P.tile_cnt[u]; s++)
+          for (int r = 0; r < 3; r++) {
+            const uint32_t v = (P.lnb[s] >> (r * evp::kLnbBits)) & evp::kLnbMask;
+            if (v & evp::kStrPrev) {
+              const uint32_t w = evp::kStrPrev | ((v + 1) & 255u);
+              P.lnb[s] = (P.lnb[s] & ~(evp::kLnbMask << (r * evp::kLnbBits))) |
+                         (w << (r * evp::kLnbBits));
+              return true;
+            }
+          }
+      }
+      return false;
+    }
     default: return false;
   }
 }
@@ -51,7 +80,7 @@ bool plant(evp::TilePlan &P, int kind) {
 
 extern "C" {
 
-int shim_kinds(void) { return 13; }
+int shim_kinds(void) { return 16; }
 
 // 1-based neighbour vectors as evp1d_init takes them.  Returns the number of
 // violations found (0 for kind 0 on a good plan), or -1 if the mistake could
@@ -65,7 +94,7 @@ long long shim_plan_check(int na, int navel, const int32_t *const idx[6], int ma
     nbp[k] = nb0.data() + (size_t)k * na;
   }
   evp::TilePlan plan;
-  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, max_tile);
+  evp::build_tile_plan(na, navel, nbp, nullptr, nullptr, &plan, max_tile, 4);
   if (kind != 0 && !plant(plan, kind)) return -1;
   std::string first;
   const long long bad = evp::verify_tile_plan(plan, nbp, max_tile, &first);

@@ -315,6 +315,19 @@ def test_smaller_tiles_bitwise(oracle_mod, points):
     assert_same(fs, oracle_run(oracle_mod, pr, 13), pr)
 
 
+@pytest.mark.parametrize("strip_w,runs", [(1, 148), (7, 3), (48, 1), (48, 148), (128, 17)])
+def test_plan_shapes_bitwise(oracle_mod, monkeypatch, strip_w, runs):
+    """Strip widths and run counts (EVP1D_STRIP_W, EVP1D_RUNS) move the run
+    boundaries, where a tile loses its previous table, and the share of
+    points recomputed as forward halo: one-column strips recompute every
+    nw/sw neighbour, one run chains every tile to its predecessor.  The bits
+    stay the oracle's."""
+    pr = synth.to_1d(synth.make_grid(131, 77, seed=9, ndte=7, curvilinear=True))
+    monkeypatch.setenv("EVP1D_STRIP_W", str(strip_w))
+    monkeypatch.setenv("EVP1D_RUNS", str(runs))
+    assert_same(gpu_run(pr, 7), oracle_run(oracle_mod, pr, 7), pr)
+
+
 def test_tile_size_tuner():
     """evp1d.tune_tile_points times each candidate on the caller's problem
     (single and batched) and leaves the fastest set."""
