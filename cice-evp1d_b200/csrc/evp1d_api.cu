@@ -109,7 +109,9 @@ void launch_sub(evp1d_t *h, int from, bool last) {
     evp::TmaArgs a = evp::problem_tma_args(h->d, from);
     a.prefetch = h->prefetch;
     a.trace = h->trace;
-    evp::launch_tma(a, h->p, last, h->d.stream);
+    a.nsub = 1;
+    a.last = last;
+    evp::launch_tma(a, h->p, h->d.stream);
   } else {
     evp::launch_fused(evp::problem_fused_args(h->d, from), h->p, last, h->d.stream);
   }
@@ -296,6 +298,14 @@ int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6]
     delete h;
     return rc;
   }
+  // EVP1D_PERSIST=1: a call's subcycles in one launch where the device keeps
+  // every run's CTA resident (asked after problem_create has allowed the
+  // kernel's shared memory).  Off by default: on grid1600x1200 it measured
+  // 276 us per subcycle against 101 for one launch per subcycle, because a
+  // run's first tile waits for the neighbouring runs' last tiles of the
+  // subcycle before (the strip order chains the runs).
+  if (const char *e = getenv("EVP1D_PERSIST"))
+    h->persist = atoi(e) != 0 && evp::tma_can_persist(device, plan.nruns);
   *handle = h;
   return EVP1D_OK;
 }
@@ -493,6 +503,19 @@ int evp1d_subcycles(evp1d_t *h, int ndte) {
   if (h->d.ntiles == 0 || ndte == 0) return EVP1D_OK;
   CHECK(select_device(h));
   cudaStream_t st = h->d.stream;
+  if (h->path == kPathTma && h->persist && ndte > 1) {
+    // the whole call in one launch; the per-tile counters start at zero
+    CUDA_TRY(cudaMemsetAsync(h->d.epoch, 0, sizeof(unsigned) * (size_t)h->d.ntiles, st));
+    evp::TmaArgs a = evp::problem_tma_args(h->d, h->d.cur);
+    a.trace = h->trace;
+    a.nsub = ndte;
+    a.last = true;
+    a.epoch = h->d.epoch;
+    CUDA_TRY(evp::launch_tma(a, h->p, st));
+    if (ndte & 1) h->d.cur = 1 - h->d.cur;
+    h->launches++;
+    return EVP1D_OK;
+  }
   int body = ndte - 1;  // subcycles before the last one
   while (body >= kGraphChunk) {
     const int c = h->d.cur;
@@ -591,6 +614,19 @@ int evp1d_debug_wait_timeout(evp1d_t *h, long long ns) {
   return EVP1D_OK;
 }
 
+int evp1d_debug_dep_wait_timeout(evp1d_t *h, long long ns) {
+  if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
+  if (ns < 1000000 || ns > 1000000000)
+    return fail(EVP1D_ERR_INVALID_ARG, "wait limit %lld ns outside [1e6, 1e9]", ns);
+  if (h->d.ntiles == 0) return fail(EVP1D_ERR_STATE, "the problem has no tiles");
+  CUDA_TRY(cudaSetDevice(h->d.device));
+  // the first tile's counter, zeroed here and raised by no kernel meanwhile
+  CUDA_TRY(cudaMemsetAsync(h->d.epoch, 0, sizeof(unsigned), h->d.stream));
+  evp::launch_dep_probe(h->d.err, h->d.epoch, (unsigned long long)ns, h->d.stream);
+  CUDA_TRY(cudaGetLastError());
+  return EVP1D_OK;
+}
+
 int evp1d_debug_fail_alloc(int n) {
   if (n < 0) return fail(EVP1D_ERR_INVALID_ARG, "n = %d < 0", n);
   g_fail_alloc.store(n);
@@ -644,18 +680,24 @@ int evp1d_autotune(evp1d_t *h, int nsub, char *chosen, int len) {
   copy_all(true);
   struct Cand {
     int path, prefetch;
+    bool persist;
   };
-  const Cand cands[] = {{kPathTma, 0}, {kPathTma, 2}, {kPathFused, 0}};
+  // the multi-subcycle launch (EVP1D_PERSIST) stays a caller's choice: it is
+  // far slower with the strip-ordered runs
+  const Cand all[] = {{kPathTma, 0, false}, {kPathTma, 2, false}, {kPathFused, 0, false}};
+  std::vector<Cand> cands(all, all + 3);
   const int old_path = h->path, old_pf = h->prefetch;
+  const bool old_persist = h->persist;
   int best = -1;
   float best_ms = 0.f;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   int rc = EVP1D_OK;
-  for (int c = 0; c < 3 && rc == EVP1D_OK; c++) {
+  for (int c = 0; c < (int)cands.size() && rc == EVP1D_OK; c++) {
     h->path = cands[c].path;
     h->prefetch = cands[c].prefetch;
+    h->persist = cands[c].persist;
     drop_graphs(h);
     rc = evp1d_subcycles(h, 2);  // warm-up (also builds nothing: < one chunk)
     if (rc == EVP1D_OK) {
@@ -687,15 +729,17 @@ int evp1d_autotune(evp1d_t *h, int nsub, char *chosen, int len) {
   if (rc != EVP1D_OK || best < 0) {
     h->path = old_path;
     h->prefetch = old_pf;
+    h->persist = old_persist;
     return rc != EVP1D_OK ? rc : fail(EVP1D_ERR_CUDA, "autotune found no candidate");
   }
   CHECK(check_device_error(h));
   h->path = cands[best].path;
   h->prefetch = cands[best].prefetch;
+  h->persist = cands[best].persist;
   char buf[128];
-  snprintf(buf, sizeof buf, "%s prefetch=%d (%.2f us/subcycle)",
-           h->path == kPathTma ? "fused-tile-tma" : "fused-tile", h->prefetch,
-           1000.0 * best_ms / nsub);
+  snprintf(buf, sizeof buf, "%s%s prefetch=%d (%.2f us/subcycle)",
+           h->path == kPathTma ? "fused-tile-tma" : "fused-tile",
+           h->persist ? " multi-subcycle" : "", h->prefetch, 1000.0 * best_ms / nsub);
   h->tuned = buf;
   if (chosen && len > 0) {
     strncpy(chosen, buf, (size_t)len - 1);

@@ -461,15 +461,18 @@ void launch_state(evp1d_t *h, double *const s_in[12], double *const s_out[12],
   if (h->path == kPathTma) {
     TmaArgs a = problem_tma_args(d, 0);
     a.prefetch = h->prefetch;
+    // one subcycle: set 0 is only read, set 1 only written
     for (int k = 0; k < 12; k++) {
-      a.sf[7 + k] = s_in[k];
-      a.s_out[k] = s_out[k];
+      a.s[0][k] = s_in[k];
+      a.s[1][k] = s_out[k];
     }
-    a.u_in = u_in;
-    a.v_in = v_in;
-    a.u_out = u_out;
-    a.v_out = v_out;
-    launch_tma(a, h->p, last, d.stream);
+    a.u[0] = const_cast<double *>(u_in);
+    a.v[0] = const_cast<double *>(v_in);
+    a.u[1] = u_out;
+    a.v[1] = v_out;
+    a.nsub = 1;
+    a.last = last;
+    launch_tma(a, h->p, d.stream);
   } else {
     FusedArgs a = problem_fused_args(d, 0);
     for (int k = 0; k < 12; k++) {
@@ -484,7 +487,45 @@ void launch_state(evp1d_t *h, double *const s_in[12], double *const s_out[12],
   }
 }
 
+// `len` forward subcycles from tape entry e0: the velocities of subcycle i go
+// into entry e0 + i + 1, the stresses alternate between s0 and s1 (s0 holds
+// the start).  One multi-subcycle launch where the handle runs those, else one
+// launch per subcycle.
+void launch_states(evp1d_t *h, double *const s0[12], double *const s1[12], double *tu0,
+                   double *tv0, size_t entry_step, int len, bool last);
+
 double *tape_u(AdjointState &A, int e) { return A.tape + (size_t)e * 2 * A.stride; }
+
+void launch_states(evp1d_t *h, double *const s0[12], double *const s1[12], double *tu0,
+                   double *tv0, size_t entry_step, int len, bool last) {
+  DeviceProblem &d = h->d;
+  if (len <= 0) return;
+  if (h->path == kPathTma && h->persist && len > 1) {
+    cudaMemsetAsync(d.epoch, 0, sizeof(unsigned) * (size_t)d.ntiles, d.stream);
+    TmaArgs a = problem_tma_args(d, 0);
+    for (int k = 0; k < 12; k++) {
+      a.s[0][k] = s0[k];
+      a.s[1][k] = s1[k];
+    }
+    a.u[0] = tu0;
+    a.v[0] = tv0;
+    a.uv_step = entry_step;
+    a.nsub = len;
+    a.last = last;
+    a.epoch = d.epoch;
+    launch_tma(a, h->p, d.stream);
+    h->launches++;
+    return;
+  }
+  for (int i = 0; i < len; i++) {
+    const bool odd = i & 1;
+    launch_state(h, odd ? s1 : s0, odd ? s0 : s1, tu0 + (size_t)i * entry_step,
+                 tv0 + (size_t)i * entry_step, tu0 + (size_t)(i + 1) * entry_step,
+                 tv0 + (size_t)(i + 1) * entry_step, last && i == len - 1);
+  }
+  h->launches += len;
+}
+
 double *tape_v(AdjointState &A, int e) { return A.tape + (size_t)e * 2 * A.stride + A.stride; }
 double *ck_u(AdjointState &A, int j) {
   return A.ck + (size_t)j * (2 * A.stride + 12 * A.sstride);
@@ -606,14 +647,9 @@ int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
                             cudaMemcpyDeviceToDevice, st));
     ADJ_TRY(cudaMemcpyAsync(tape_v(A, 0), d.v[c], sizeof(double) * d.nuv,
                             cudaMemcpyDeviceToDevice, st));
-    int b = c;
-    for (int n = n_cp; n < ndte; n++) {
-      const int e = n - n_cp;
-      launch_state(h, d.stress[b], d.stress[1 - b], tape_u(A, e), tape_v(A, e),
-                   tape_u(A, e + 1), tape_v(A, e + 1), n == ndte - 1);
-      b = 1 - b;
-    }
-    h->launches += ndte - n_cp;
+    launch_states(h, d.stress[c], d.stress[1 - c], tape_u(A, 0), tape_v(A, 0), 2 * A.stride,
+                  ndte - n_cp, true);
+    const int b = ((ndte - n_cp) & 1) ? 1 - c : c;
     // the final state back into the handle's buffers for evp1d_download
     ADJ_TRY(cudaMemcpyAsync(d.u[b], tape_u(A, ndte - n_cp), sizeof(double) * d.nslots,
                             cudaMemcpyDeviceToDevice, st));
@@ -723,12 +759,10 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
                               cudaMemcpyDeviceToDevice, st));
     // recompute the segment's velocities from its checkpoint
     const int e0 = A.seg_base;
-    for (int i = 0; i < len; i++) {
-      const int b = i & 1;
-      launch_state(h, A.spp[b], A.spp[1 - b], tape_u(A, e0 + i), tape_v(A, e0 + i),
-                   tape_u(A, e0 + i + 1), tape_v(A, e0 + i + 1), false);
-      launches++;
-    }
+    const long long before = h->launches;
+    launch_states(h, A.spp[0], A.spp[1], tape_u(A, e0), tape_v(A, e0), 2 * A.stride, len, false);
+    launches += h->launches - before;
+    h->launches = before;
     for (int i = len - 1; i >= 0; i--)
       reverse_step(tape_u(A, e0 + i), tape_v(A, e0 + i), tape_u(A, e0 + i + 1),
                    tape_v(A, e0 + i + 1));

@@ -26,6 +26,9 @@ struct evp1d_handle {
   evp::Params p{};
   int path = kPathTma;
   int prefetch = 0;  // L2 prefetch distance of the TMA kernel (tiles)
+  // TMA path: a call's subcycles in one launch whose CTAs stay resident
+  // (cooperative), instead of one launch per subcycle in CUDA graphs
+  bool persist = false;
   long long *trace = nullptr;  // device timing trace (EVP1D_TRACE, debug)
   bool uploaded = false;
   bool uinit_explicit = false;  // the last upload gave uvel_init/vvel_init

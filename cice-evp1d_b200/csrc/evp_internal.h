@@ -63,6 +63,8 @@ struct DeviceProblem {
   uint32_t *lcor = nullptr;  // packed stress corner velocity indices
   uint32_t *halo_lcc = nullptr, *halo_lcor = nullptr;
   int32_t *uvx_off = nullptr, *uvx_cnt = nullptr, *uvx_idx = nullptr;
+  int32_t *dep_off = nullptr, *dep_idx = nullptr;  // subcycle dependencies (TilePlan)
+  unsigned *epoch = nullptr;     // per-tile counters of a multi-subcycle launch
   int32_t *tile_meta = nullptr;  // 8 int32 per tile (see TmaArgs)
   int32_t *tile_rec = nullptr;   // kRecInts int32 per tile (producer records)
   double *cblk = nullptr;        // per-call constants, kConstFields x 256 per tile

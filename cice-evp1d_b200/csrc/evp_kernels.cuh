@@ -100,13 +100,29 @@ struct TmaArgs {
   const int32_t *tile_meta = nullptr;
   // per tile one producer record of kRecInts int32 (evp_tiles.h)
   const int32_t *tile_rec = nullptr;
-  const double *sf[kTmaStressFields] = {};
+  // dxT, dyT, HTE, HTN, HTEm1, HTNm1, strength (the halo's static gathers)
+  const double *sg[7] = {};
   const double *cblk = nullptr;  // constant blocks, kConstFields x kTileOwned per tile
-  const double *u_in = nullptr, *v_in = nullptr;
-  double *u_out = nullptr, *v_out = nullptr;
-  double *s_out[12] = {};
+  // the ping-pong state: subcycle k of a launch reads set (k & 1) and writes
+  // set (k & 1) ^ 1 (a one-subcycle launch never writes set 0)
+  double *u[2] = {}, *v[2] = {};
+  double *s[2][12] = {};
+  // written on the launch's last subcycle when `last` is set
   double *strintx = nullptr, *strinty = nullptr, *Cb = nullptr;
   double *str_out[8] = {};
+  int nsub = 1;        // subcycles of this launch
+  bool last = false;   // the launch's last subcycle is the call's last
+  // Tape mode (uv_step > 0): subcycle k reads u[0] + k * uv_step and writes
+  // u[0] + (k + 1) * uv_step (v likewise), so that every subcycle's
+  // velocities stay in memory (the adjoint's tape entries); the stresses
+  // still alternate between s[0] and s[1].
+  size_t uv_step = 0;
+  // A launch of several subcycles: per tile a counter that each consumer warp
+  // raises by one when it is done with the tile in a subcycle (zeroed before
+  // the launch), and the tiles each tile waits for (evp_tiles.h dep_off /
+  // dep_idx) before it loads the next subcycle's state.
+  unsigned *epoch = nullptr;
+  const int32_t *dep_off = nullptr, *dep_idx = nullptr;
   int *err = nullptr;  // nonzero after a bounded wait ran out
   int prefetch = 0;    // tiles prefetched into L2 ahead of the shared ring
   // optional timing trace of block 0 (debug): per tile 8 %globaltimer stamps
@@ -127,8 +143,18 @@ const char *tma_wait_name(int code);
 // One bounded wait on an mbarrier that nothing completes: it runs out after
 // limit_ns and leaves its code in *err (a check of the timeout path).
 void launch_wait_probe(int *err, unsigned long long limit_ns, cudaStream_t st);
-// One CTA per run (grid = nruns, at most one per SM).
-void launch_tma(const TmaArgs &a, const Params &p, bool last, cudaStream_t st);
+// The same for the counter wait of a multi-subcycle launch: one wait on
+// *counter (which must stay 0) that runs out after limit_ns.
+void launch_dep_probe(int *err, const unsigned *counter, unsigned long long limit_ns,
+                      cudaStream_t st);
+// One CTA per run (grid = nruns, at most one per SM).  A launch of several
+// subcycles (a.nsub > 1, a.epoch set) keeps its CTAs across the subcycles and
+// needs them all resident at once: it is a cooperative launch.  Returns the
+// launch's error.
+cudaError_t launch_tma(const TmaArgs &a, const Params &p, cudaStream_t st);
+// Whether this device runs several subcycles per launch (cooperative launch
+// with one CTA per run resident on every SM).
+bool tma_can_persist(int device, int nruns);
 
 // ---- layout conversion between the reference 1D order and slots ----------
 constexpr int kMaxBatch = 32;

@@ -1,32 +1,29 @@
-// evp_kernels_tma.cu -- the fused EVP subcycle as a persistent, TMA-fed
-// producer/consumer kernel (sm_100a).
+// evp_kernels_tma.cu -- the fused EVP subcycle as a TMA-fed producer/consumer
+// kernel (sm_100a), one CTA per SM.
 //
 // CTA b works through the tiles of its run, t = run_off[b] .. run_off[b+1]-1,
-// in order (one CTA per SM).  A tile's inputs are staged in shared memory in
-// two parts with different lifetimes:
-//   - the stress part (geometry, strength, packed index words, the 12
-//     stresses, u and v of the owned points and of the stencil's extra
-//     points, and the recomputed forward halo) is dead once stress is done;
-//     it has a two-slot ring, so one later tile loads while one computes;
-//   - the stepu part (the 13 stepu inputs) has one slot, loaded while the
-//     consumers compute the tile's stress.
-// The owned points of a tile are contiguous slots and its per-call constants
-// one contiguous block, so the owned data arrive by cp.async.bulk (TMA)
-// copies completing on the slot's mbarrier (complete_tx); the halo and the
-// extra velocities are gathered with 4/8-byte cp.async, whose completion
-// arrives on the same mbarrier (cp.async.mbarrier.arrive).
-// Producer warps: the bulk warp (the bulk copies of both parts) and
-// kGatherWarps gather warps issuing the cp.async gathers side by side with it.  The producers' own inputs -- the
-// tile's slot range and gather lists -- are one 1.3 KB record per tile that a
-// bulk copy brings kRecRing tiles ahead, so no producer waits on a global
-// load.
+// in order.  A tile's stress inputs (geometry, strength, packed index words,
+// the 12 stresses, u and v of the owned points and of the stencil's extra
+// points, and the recomputed forward halo) are staged in shared memory in a
+// two-slot ring, so one later tile loads while one computes.  The owned
+// points of a tile are contiguous slots and its per-call constants one
+// contiguous block, so the owned data arrive by cp.async.bulk (TMA) copies
+// completing on the slot's mbarrier (complete_tx); the halo and the extra
+// velocities are gathered with 4/8-byte cp.async, whose completion arrives on
+// the same mbarrier (cp.async.mbarrier.arrive).
+// Producer warps: the bulk warp (the bulk copies) and kGatherWarps gather
+// warps issuing the cp.async gathers side by side with it.  The producers'
+// own inputs -- the tile's slot range and gather lists -- are one 1.3 KB
+// record per tile that a bulk copy brings kRecRing tiles ahead, so no
+// producer waits on a global load.
 // Eight consumer warps (one thread per compute-set point: the tile's owned
 // points, then its forward halo, 256 at most) compute stress from shared
 // memory into the tile's str table, then stepu for the owned points, writing
 // the new stresses and velocities to the other ping-pong buffer.  Stepu reads
 // str from the tile's own table and from the previous tile's, which stays
 // alive: three str tables rotate, so that one tile's stress can start while
-// stepu still reads the two before it.
+// stepu still reads the two before it.  The 13 stepu inputs of a point come
+// straight from its constant block into the thread's registers, a tile ahead.
 //
 // Every mbarrier wait is bounded by %globaltimer (kWaitNs): on expiry the
 // kernel records an error code, every thread of the consumer group leaves the
@@ -63,13 +60,13 @@ struct SSlot {
   int hdr[4];  // tile offset, owned count, halo count (written by the bulk warp)
 };
 
+static_assert(kConstTileSlots == kTileOwned, "constant blocks hold one tile");
+static_assert(kConstFields == kConstStressFields + kTmaStepuFields, "constant block layout");
+
 // Stepu part of a tile: constant block fields 8..20 (one bulk copy).
 struct USlot {
   double cu[kTmaStepuFields][kTileOwned];
 };
-
-static_assert(kConstTileSlots == kTileOwned, "constant blocks hold one tile");
-static_assert(kConstFields == kConstStressFields + kTmaStepuFields, "constant block layout");
 
 struct Smem {
   SSlot ss[kSSlots];
@@ -78,14 +75,13 @@ struct Smem {
   int32_t rec[kRecRing][kRecInts];
   unsigned long long sfull[kSSlots];
   unsigned long long sempty[kSSlots];
-  unsigned long long ufull, uempty;
   unsigned long long rec_full[kRecRing];
+  unsigned long long ufull, uempty;
   int abort_flag;
   int prod_ok;  // the bulk warp's waits succeeded for the current tile
 };
 
-static_assert(sizeof(SSlot) % 16 == 0 && sizeof(USlot) % 16 == 0,
-              "slots must keep 16-byte alignment");
+static_assert(sizeof(SSlot) % 16 == 0, "slots must keep 16-byte alignment");
 static_assert((kRecInts * 4) % 16 == 0, "records are bulk-copied");
 static_assert(sizeof(Smem) <= 227 * 1024, "shared memory per block");
 
@@ -118,6 +114,19 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t 
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Non-blocking test whether the phase of parity `parity` has completed.
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(smem_addr(bar)), "r"(parity)
@@ -208,17 +217,54 @@ __device__ __forceinline__ void trace_stamp(const TmaArgs &a, int it, int slot) 
   if (a.trace && blockIdx.x == 0 && it < kTraceTiles) a.trace[it * 8 + slot] = (long long)global_ns();
 }
 
-// The stepu part of tile t (constant block fields 8..20) into the stepu slot.
-__device__ __forceinline__ void issue_stepu(const TmaArgs &a, Smem &S, int t) {
-  constexpr uint32_t kBytes = kTmaStepuFields * kTileOwned * 8u;
-  mbar_arrive_expect_tx(&S.ufull, kBytes);
-  bulk_g2s(S.us.cu, a.cblk + ((size_t)t * kConstFields + kConstStressFields) * kTileOwned, kBytes,
-           &S.ufull);
+// Acquire load of a counter another CTA raises (gpu scope).
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
+// Order this thread's generic-proxy global accesses with its async-proxy
+// (bulk copy) accesses of global memory.
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
+// Bounded wait until the counter *e, which other CTAs raise, reaches `need`
+// (acquire); on expiry the wait's code goes into the error word.
+__device__ __forceinline__ bool wait_counter(const unsigned *e, unsigned need, int *err,
+                                             int code, unsigned long long limit_ns) {
+  if (ld_acquire(e) >= need) return true;
+  const unsigned long long t0 = global_ns();
+  while (ld_acquire(e) < need) {
+    if (global_ns() - t0 > limit_ns) {
+      atomicMax(err, code);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Relaxed load of a counter another CTA raises (gpu scope, past L1).
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Coherent 8-byte load (at L2) of state other CTAs may have written.
+__device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
+
 // ---------------- the kernel ---------------------------------------------------
-// kStd: parameters with std_params(p) (stress_update_std).
-template <bool kLast, bool kStd>
+// kStd: parameters with std_params(p) (stress_update_std).  The launch runs
+// a.nsub subcycles; CTA b works through its run's tiles once per subcycle.
+// kMulti: a launch of several subcycles (a.nsub > 1 with per-tile counters);
+// otherwise one subcycle, whose last-subcycle outputs kLast selects.
+template <bool kLast, bool kStd, bool kMulti>
 __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   // Indexed straight off the __shared__ symbol (no integer round trip), so
   // every access compiles to a shared-memory load or store, not a generic one.
@@ -236,9 +282,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       mbar_init(&S.sfull[s], 1 + 32 * kGatherWarps);  // expect_tx arrival + cp.async lanes
       mbar_init(&S.sempty[s], 1);                     // one consumer arrival per use
     }
+    for (int r = 0; r < kRecRing; r++) mbar_init(&S.rec_full[r], 1);
     mbar_init(&S.ufull, 1);
     mbar_init(&S.uempty, kConsumers / 32);  // one arrival per consumer warp
-    for (int r = 0; r < kRecRing; r++) mbar_init(&S.rec_full[r], 1);
     S.abort_flag = 0;
     mbar_fence_init();
   }
@@ -246,42 +292,85 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   __syncthreads();
 
   const int T0 = a.run_off[blockIdx.x], T1 = a.run_off[blockIdx.x + 1];
+  const int n = T1 - T0;             // tiles of the run
+  const int nq = kMulti ? n * a.nsub : n;  // (subcycle, tile) steps of the launch
+  constexpr bool multi = kMulti;
   constexpr uint32_t kCsBytes = kConstStressFields * kTileOwned * 8u;
   constexpr size_t kBlk = (size_t)kConstFields * kTileOwned;  // doubles per constant block
+  if (n <= 0) return;
 
   if (tid >= kConsumers) {
     // ======================= producers ===================================
     // The bulk warp (pw 0) waits for the tile record and the free slot,
     // writes the slot header, arms the slot's full barrier and issues the
-    // bulk copies (TMA unit); the gather warps meanwhile issue the 8-byte
-    // cp.async gathers of the forward halo and the extra velocities
-    // (load/store path).  Two named-barrier handshakes per tile order the
-    // warps: after the first the slot is armed and the record readable, after
-    // the second every warp is done with the record, which the bulk warp then
-    // refills.  The bulk warp's waits are bounded and it reaches the first
-    // handshake on every path, so the handshakes cannot hang; a failed wait
-    // is passed on through prod_ok.
-    // The bulk warp also issues the stepu part: tile i's stress part goes
-    // out two tiles ahead of its use, tile j's stepu part as soon as the
-    // stepu slot is free (end of stepu(j-1)).  The TMA unit serves the
-    // copies in issue order, so in round i the stepu part of tile i-2 is
-    // issued before the stress part of tile i (whose slot was freed earlier,
-    // at the end of stress(i-3)), which keeps the urgent copy at the front.
+    // bulk copies (TMA unit); the gather warps meanwhile gather the forward
+    // halo and the extra velocities (8-byte cp.async, or, in a launch of
+    // several subcycles, coherent loads).  Two named-barrier handshakes per
+    // step order the warps: after the first the slot is armed and the record
+    // readable, after the second every warp is done with the record, which
+    // the bulk warp then refills.  The bulk warp's waits are bounded and it
+    // reaches the first handshake on every path, so the handshakes cannot
+    // hang; a failed wait is passed on through prod_ok.
+    // Step q = (subcycle q / n, tile q % n).  In round q the bulk warp first
+    // issues step q-1's stepu part (once stepu of step q-2 has freed the
+    // stepu slot), then step q's stress part (once stress of step q-2 has
+    // freed its slot).  The TMA unit serves copies in issue order, which keeps
+    // the part needed first at the front.
+    // A launch of several subcycles: step q's stress part goes out only when
+    // every tile its tile depends on has finished the previous subcycle.  Its
+    // lanes read those tiles' counters (relaxed) at the end of round q-1 and
+    // check them here, so the check usually costs no wait; the acquire fence
+    // then orders the state reads after the counters.  The bulk warp also
+    // publishes this CTA's steps: once stepu of a step is done (all consumer
+    // warps arrived on the stepu slot's barrier), it raises the tile's
+    // counter after a gpu-scope fence, at the end of a round, where the wait
+    // for the next slot absorbs the fence.  Every step's stepu part is out
+    // before a round can wait on counters, so consumers finish every earlier
+    // step without this round: no wait can depend on itself.
     const int pw = (tid - kConsumers) >> 5;
     const int lane = tid & 31;
     constexpr uint32_t kRecBytes = kRecInts * 4u;
+    constexpr uint32_t kUBytes = kTmaStepuFields * kTileOwned * 8u;
+    auto issue_stepu = [&](int q) {  // lane 0 of the bulk warp
+      mbar_arrive_expect_tx(&S.ufull, kUBytes);
+      bulk_g2s(S.us.cu,
+               a.cblk + ((size_t)(T0 + (kMulti ? q % n : q)) * kConstFields + kConstStressFields) *
+                            kTileOwned,
+               kUBytes, &S.ufull);
+    };
+    int pub = 0;  // steps whose counters are raised (multi-subcycle launches)
+    int nu = 0;   // stepu parts issued (the bulk warp's lane 0 counts)
+    // Lane 0: raise the counters of every step whose stepu has completed.
+    // Stepu phases below nu - 1 are known complete (the bulk warp waited for
+    // each before issuing a later stepu part); phase nu - 1, the last one
+    // issued, is tested: its parity is unambiguous because the phase after it
+    // cannot complete before the next part goes out.
+    auto publish = [&](int limit) {
+      bool any = false;
+      while (pub < limit) {
+        const bool done = pub < nu - 1 || (pub == nu - 1 && mbar_test_wait(&S.uempty, (uint32_t)pub & 1));
+        if (!done) break;
+        if (!any) __threadfence();
+        any = true;
+        atomicAdd(a.epoch + T0 + (kMulti ? pub % n : pub), 1u);
+        pub++;
+      }
+    };
     if (pw == 0 && lane == 0) {
-      for (int r = 0; r < kRecRing; r++) {
-        const int t = T0 + r;
-        if (t >= T1) break;
+      for (int r = 0; r < kRecRing && r < nq; r++) {
+        const int t = T0 + (kMulti ? r % n : r);
         mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
         bulk_g2s(S.rec[r], a.tile_rec + (size_t)t * kRecInts, kRecBytes, &S.rec_full[r]);
       }
     }
     int issued = 0;
-    int nu = 0;  // stepu parts issued (counted by the bulk warp's lane 0)
     bool ok = true;
-    for (int t = T0; t < T1; t++) {
+    unsigned seen = 0u;  // per lane: the smallest counter polled for the next step
+    for (int q = 0; q < nq; q++) {
+      const int sub = kMulti ? q / n : 0, t = T0 + (kMulti ? q % n : q);
+      const int from = sub & 1;
+      const double *u_in = kMulti && a.uv_step ? a.u[0] + (size_t)sub * a.uv_step : a.u[from];
+      const double *v_in = kMulti && a.uv_step ? a.v[0] + (size_t)sub * a.uv_step : a.v[from];
       const int r = issued % kRecRing;
       const int s = issued % kSSlots;
       const uint32_t use = (uint32_t)(issued / kSSlots);
@@ -293,14 +382,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
           w = mbar_wait(&S.rec_full[r], (uint32_t)(issued / kRecRing) & 1, a.err, 6) ? 1 : 0;
           trace_stamp(a, issued, 3);
           if (w && issued >= kSSlots) {
-            // stepu part nu == issued - 2; its slot frees after stepu(nu - 1)
+            // step q-1's stepu part; the slot frees after stepu of step q-2
             w = mbar_wait(&S.uempty, (uint32_t)(nu - 1) & 1, a.err, 9) ? 1 : 0;
-            if (w) issue_stepu(a, S, T0 + (nu++));
+            if (w) issue_stepu(nu++);
             if (w) w = mbar_wait(&S.sempty[s], (use - 1) & 1, a.err, 2) ? 1 : 0;
           }
-          trace_stamp(a, issued, 4);
         }
         w = __shfl_sync(0xffffffffu, w, 0);
+        if (w && multi && sub > 0) {
+          // the tiles step q depends on have finished subcycle sub - 1; the
+          // warp waits together, lane 0 publishing this CTA's finished steps
+          // meanwhile (a tile may wait on its own run's steps)
+          const unsigned need = (unsigned)sub;
+          const int d0 = a.dep_off[t], d1 = a.dep_off[t + 1];
+          const unsigned long long t0 = global_ns();
+          for (bool first = true;; first = false) {
+            bool mine = true;
+            for (int d = d0 + lane; d < d1 && mine; d += 32) {
+              if (first && d < d0 + 32 && seen >= need) continue;
+              mine = ld_relaxed(a.epoch + a.dep_idx[d]) >= need;
+            }
+            if (__all_sync(0xffffffffu, mine)) break;
+            if (lane == 0) publish(q);
+            // one decision for the whole warp (lane 0's clock)
+            if (__shfl_sync(0xffffffffu, global_ns() - t0 > kWaitNs ? 1 : 0, 0)) {
+              if (lane == 0) atomicMax(a.err, 13);
+              w = 0;
+              break;
+            }
+          }
+          // acquire: the neighbours' state is read after their counters, by
+          // these bulk copies (async proxy) and by the gather warps
+          fence_acq_rel_gpu();
+          fence_proxy_async_global();
+        }
+        if (lane == 0) trace_stamp(a, issued, 4);
         if (w) {
           const int nh = rec[3];
           for (int h = lane; h < nh; h += 32) {
@@ -333,31 +449,48 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
         if (lane == 0)
           bulk_g2s(st.cs, a.cblk + (size_t)t * kBlk, kCsBytes, &S.sfull[s]);
         else if (lane <= 12)
-          bulk_g2s(st.s12[lane - 1], a.sf[6 + lane] + off, b8, &S.sfull[s]);
+          bulk_g2s(st.s12[lane - 1], a.s[from][lane - 1] + off, b8, &S.sfull[s]);
         else if (lane == 13)
-          bulk_g2s(st.u, a.u_in + off, b8, &S.sfull[s]);
+          bulk_g2s(st.u, u_in + off, b8, &S.sfull[s]);
         else if (lane == 14)
-          bulk_g2s(st.v, a.v_in + off, b8, &S.sfull[s]);
+          bulk_g2s(st.v, v_in + off, b8, &S.sfull[s]);
         if (lane == 0) {
-          if (issued == 0) issue_stepu(a, S, T0 + (nu++));
+          if (issued == 0) issue_stepu(nu++);
           trace_stamp(a, issued, 6);
         }
       } else {
         // gather warp gw takes the velocity extras u (first) / v (last) and
         // every kGatherWarps-th halo field; the last one also the halo meta
         const int gw = pw - 1;
-        if (gw == 0)
-          for (int x = lane; x < nx; x += 32)
-            cp_async8(&st.u[kTileOwned + x], a.u_in + rec[kRecUvx + x]);
-        if (gw == kGatherWarps - 1)
-          for (int x = lane; x < nx; x += 32)
-            cp_async8(&st.v[kTileOwned + x], a.v_in + rec[kRecUvx + x]);
-        for (int h = lane; h < nh; h += 32) {
-          const int g = rec[kRecHalo + h];
-          for (int f = gw; f < kTmaStressFields; f += kGatherWarps) cp_async8(&st.hf[f][h], a.sf[f] + g);
-          if (gw == kGatherWarps - 1) cp_async4(&st.hmeta[h], a.meta + g);
+        if (!multi) {
+          if (gw == 0)
+            for (int x = lane; x < nx; x += 32)
+              cp_async8(&st.u[kTileOwned + x], u_in + rec[kRecUvx + x]);
+          if (gw == kGatherWarps - 1)
+            for (int x = lane; x < nx; x += 32)
+              cp_async8(&st.v[kTileOwned + x], v_in + rec[kRecUvx + x]);
+          for (int h = lane; h < nh; h += 32) {
+            const int g = rec[kRecHalo + h];
+            for (int f = gw; f < kTmaStressFields; f += kGatherWarps)
+              cp_async8(&st.hf[f][h], (f < 7 ? a.sg[f] : a.s[from][f - 7]) + g);
+            if (gw == kGatherWarps - 1) cp_async4(&st.hmeta[h], a.meta + g);
+          }
+          cp_async_arrive(&S.sfull[s]);
+        } else {
+          // state written by other CTAs in this launch: loads at L2 (not a
+          // copy that an earlier read may have left in this SM's L1)
+          if (gw == 0)
+            for (int x = lane; x < nx; x += 32) st.u[kTileOwned + x] = ld_cg(u_in + rec[kRecUvx + x]);
+          if (gw == kGatherWarps - 1)
+            for (int x = lane; x < nx; x += 32) st.v[kTileOwned + x] = ld_cg(v_in + rec[kRecUvx + x]);
+          for (int h = lane; h < nh; h += 32) {
+            const int g = rec[kRecHalo + h];
+            for (int f = gw; f < kTmaStressFields; f += kGatherWarps)
+              st.hf[f][h] = ld_cg((f < 7 ? a.sg[f] : a.s[from][f - 7]) + g);
+            if (gw == kGatherWarps - 1) st.hmeta[h] = a.meta[g];
+          }
+          mbar_arrive(&S.sfull[s]);
         }
-        cp_async_arrive(&S.sfull[s]);
         if (gw == 0 && lane == 0) trace_stamp(a, issued, 7);
       }
       // the record's generic reads come before its async-proxy refill
@@ -365,12 +498,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       stage_sync();  // handshake 2
       if (pw == 0) {
         if (lane == 0) trace_stamp(a, issued, 0);
-        const int tr = t + kRecRing;
-        if (lane == 0 && tr < T1) {
+        const int qr = q + kRecRing;
+        if (lane == 0 && qr < nq) {
           mbar_arrive_expect_tx(&S.rec_full[r], kRecBytes);
-          bulk_g2s(S.rec[r], a.tile_rec + (size_t)tr * kRecInts, kRecBytes, &S.rec_full[r]);
+          bulk_g2s(S.rec[r], a.tile_rec + (size_t)(T0 + (kMulti ? qr % n : qr)) * kRecInts, kRecBytes,
+                   &S.rec_full[r]);
         }
-        if (a.prefetch > 0) {
+        if (a.prefetch > 0 && !multi) {
           const int tp = t + a.prefetch;
           if (tp < T1 && lane < 15) {
             // what the stage load of a later tile copies: its constant block,
@@ -380,9 +514,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
             if (lane == 0)
               bulk_prefetch_l2(a.cblk + (size_t)tp * kBlk, (uint32_t)(kBlk * 8u));
             else if (lane <= 12)
-              bulk_prefetch_l2(a.sf[6 + lane] + po, pb);
+              bulk_prefetch_l2(a.s[from][lane - 1] + po, pb);
             else
-              bulk_prefetch_l2((lane == 13 ? a.u_in : a.v_in) + po, pb);
+              bulk_prefetch_l2((lane == 13 ? u_in : v_in) + po, pb);
+          }
+        }
+        if (multi) {
+          if (lane == 0) publish(q);
+          // the counters of the next step's dependencies, read ahead
+          const int q1 = q + 1;
+          if (q1 < nq && q1 / n > 0) {
+            const int t1 = T0 + q1 % n, d = a.dep_off[t1] + lane;
+            seen = d < a.dep_off[t1 + 1] ? ld_relaxed(a.epoch + a.dep_idx[d]) : 0u;
           }
         }
       }
@@ -390,13 +533,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     }
     if (pw == 0) {
       if (ok && lane == 0) {
-        // the stepu parts of the last tiles
+        // the stepu parts of the last steps
         for (; nu < issued; nu++) {
           if (!mbar_wait(&S.uempty, (uint32_t)(nu - 1) & 1, a.err, 9)) break;
-          issue_stepu(a, S, T0 + nu);
+          issue_stepu(nu);
         }
       }
       if (lane == 0 && nu > 0) mbar_wait(&S.ufull, (uint32_t)(nu - 1) & 1, a.err, 10);
+      if (multi && lane == 0) {
+        // the last steps' counters (a later launch zeroes them anyway)
+        const unsigned long long t0 = global_ns();
+        while (ok && pub < issued && global_ns() - t0 < kWaitNs) publish(issued);
+      }
       if (!ok) {
         // Consumers stopped early: wait (bounded) until every issued slot has
         // landed so that no copy targets shared memory after the CTA exits.
@@ -407,11 +555,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       }
       // records issued ahead and never consumed must land before exit too
       if (lane == 0) {
-        for (int k = issued; k < issued + kRecRing; k++) {
-          const int t = T0 + k;
-          if (t >= T1) break;
+        for (int k = issued; k < issued + kRecRing && k < nq; k++)
           mbar_wait(&S.rec_full[k % kRecRing], (uint32_t)(k / kRecRing) & 1, a.err, 7);
-        }
       }
     }
     __syncwarp();
@@ -419,48 +564,57 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   }
 
   // ========================= consumers ===================================
-  // Per tile one block barrier: after stress, when the tile's str table is
+  // Per step one block barrier: after stress, when the tile's str table is
   // complete.  Stepu then runs warp by warp and each warp goes straight on to
-  // the next tile's stress, so one warp's stepu overlaps the others' stress.
-  // Stepu of tile k reads the tables of tiles k and k-1 while stress of tile
-  // k+1 writes the third; the table it writes last held tile k-2, whose
-  // readers (stepu of k-2 and k-1) every warp has finished before any passes
-  // the barrier of tile k.  The stepu slot is released by one arrival per
-  // warp.  A wait that ran out anywhere is OR-reduced at the barrier, so all
-  // consumers leave the loop together.
+  // the next step's stress, so one warp's stepu overlaps the others' stress.
+  // Stepu of step q reads the tables of steps q and q-1 while stress of step
+  // q+1 writes the third; the table it writes last held step q-2, whose
+  // readers (stepu of q-2 and q-1) every warp has finished before any passes
+  // the barrier of step q.  (The first tile of a run never reads the previous
+  // table, so nothing crosses from one subcycle to the next there.)  The
+  // stepu slot is released by one arrival per warp.  A wait that ran out
+  // anywhere is OR-reduced at the barrier, so all consumers leave the loop
+  // together.
   const int c = tid;  // compute-set index: owned c < cnt, halo cnt + h
   const int lane = tid & 31;
   bool fail = false;
-  int it = 0;
-  for (int t = T0; t < T1; t++, it++) {
-    const int s = it % kSSlots;
-    const int b = it % 3;
-    const int bp = (it + 2) % 3;  // the previous tile's table
-    const bool have = mbar_wait(&S.sfull[s], (uint32_t)(it / kSSlots) & 1, a.err, 1);
-    fail |= !have;
-    if (tid == 0) trace_stamp(a, it, 1);
-    const SSlot &st = S.ss[s];
 
-    // ---------------- phase 1: stress ------------------------------------
-    // The owned thread keeps what stepu needs from the stress part (its
-    // index word and velocity) so that the slot can be released after stress.
+
+  // What stepu of a tile needs from its stress part, kept by the owned
+  // thread so that the slot can be released after stress.
+  struct Carry {
     uint32_t m = 0;
     double uold = 0.0, vold = 0.0;
     int off = 0, cnt = 0;
+  };
+
+  // ---------------- stress of step q ---------------------------------------
+  auto stress_tile = [&](int q) -> Carry {
+    Carry cy;
+    const int s = q % kSSlots;
+    const int b = q % 3;
+    const int sub = kMulti ? q / n : 0;
+    const int to = (sub & 1) ^ 1;
+    const bool wlast = kMulti ? (a.last && sub == a.nsub - 1) : kLast;
+    const bool have = mbar_wait(&S.sfull[s], (uint32_t)(q / kSSlots) & 1, a.err, 1);
+    fail |= !have;
+    if (tid == 0) trace_stamp(a, q, 1);
+    const SSlot &st = S.ss[s];
     if (have) {
-      off = st.hdr[0];
-      cnt = st.hdr[1];
+      cy.off = st.hdr[0];
+      cy.cnt = st.hdr[1];
       const int nh = st.hdr[2];
-      const bool own = c < cnt;
-      const int h = c - cnt;
+      const bool own = c < cy.cnt;
+      const int h = c - cy.cnt;
       if (own || h < nh) {
-        uint32_t lc;
+        uint32_t m, lc;
         if (own) {
           const unsigned long long ml = (unsigned long long)__double_as_longlong(st.cs[7][c]);
           m = (uint32_t)ml;
           lc = (uint32_t)(ml >> 32);
-          uold = st.u[c];
-          vold = st.v[c];
+          cy.m = m;
+          cy.uold = st.u[c];
+          cy.vold = st.v[c];
         } else {
           m = st.hmeta[h];
           lc = st.hlcor[h];
@@ -498,29 +652,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
             stress_update(s12, out, sr, F[6 * fs], gm, p);
           if (own) {
 #pragma unroll
-            for (int k = 0; k < 12; k++) a.s_out[k][off + c] = s12[k];
+            for (int k = 0; k < 12; k++) a.s[to][k][cy.off + c] = s12[k];
           }
         }
 #pragma unroll
         for (int k = 0; k < 8; k++) S.str[b][k][c] = out[k];
-        if (kLast && own) {
+        if (wlast && own) {
 #pragma unroll
-          for (int k = 0; k < 8; k++) a.str_out[k][off + c] = out[k];
+          for (int k = 0; k < 8; k++) a.str_out[k][cy.off + c] = out[k];
         }
       }
     }
-    // str of this tile complete; the stress part of slot s is free again
-    const bool stop = consumer_sync_or(fail);
-    if (tid == 0) {
-      trace_stamp(a, it, 2);
-      mbar_arrive(&S.sempty[s]);
-    }
-    if (stop) break;
+    return cy;
+  };
 
-    // ---------------- phase 2: stepu on owned points, warp by warp ----------
-    const bool hu = mbar_wait(&S.ufull, (uint32_t)it & 1, a.err, 11);
+  // ---------------- stepu of step q, owned points ------------------------
+  auto stepu_tile = [&](int q, const Carry &cy) {
+    const int b = q % 3;
+    const int bp = (q + 2) % 3;  // the previous tile's table
+    const int sub = kMulti ? q / n : 0;
+    const int to = (sub & 1) ^ 1;
+    const bool wlast = kMulti ? (a.last && sub == a.nsub - 1) : kLast;
+    const bool hu = mbar_wait(&S.ufull, (uint32_t)q & 1, a.err, 11);
     fail |= !hu;
-    if (hu && c < cnt && !((m >> 30) & kSkipU)) {
+    if (hu && c < cy.cnt && !((cy.m >> 30) & kSkipU)) {
+      const uint32_t m = cy.m;
       const USlot &us = S.us;
       const double(&str)[8][kStrRow] = S.str[b];
       // a neighbour's str: own table, or the previous tile's (kStrPrev)
@@ -532,8 +688,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       const int lnw = vnw & (kStrPrev - 1), lsw = vsw & (kStrPrev - 1);
       const int lsse = vsse & (kStrPrev - 1);
       StepuIn in;
-      in.uold = uold;
-      in.vold = vold;
+      in.uold = cy.uold;
+      in.vold = cy.vold;
       in.kvrel = us.cu[0][c];
       in.uocn = us.cu[1][c];
       in.vocn = us.cu[2][c];
@@ -556,17 +712,40 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       in.s7nw = tnw[6][lnw];
       in.s8sw = tsw[7][lsw];
       const StepuOut o = stepu_point(in, p);
-      a.u_out[off + c] = o.u;
-      a.v_out[off + c] = o.v;
-      if (kLast) {
-        a.strintx[off + c] = o.strintx;
-        a.strinty[off + c] = o.strinty;
-        a.Cb[off + c] = o.Cb;
+      double *u_out = kMulti && a.uv_step ? a.u[0] + (size_t)(sub + 1) * a.uv_step : a.u[to];
+      double *v_out = kMulti && a.uv_step ? a.v[0] + (size_t)(sub + 1) * a.uv_step : a.v[to];
+      u_out[cy.off + c] = o.u;
+      v_out[cy.off + c] = o.v;
+      if (wlast) {
+        a.strintx[cy.off + c] = o.strintx;
+        a.strinty[cy.off + c] = o.strinty;
+        a.Cb[cy.off + c] = o.Cb;
       }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&S.uempty);  // this warp is done with the stepu slot
-    if (tid == 0) trace_stamp(a, it, 5);
+    if (tid == 0) trace_stamp(a, q, 5);
+  };
+
+  // the barrier after stress of step q: its str table is complete and its
+  // stress slot free again
+  auto stress_done = [&](int q) -> bool {
+    const bool stop = consumer_sync_or(fail);
+    if (tid == 0) {
+      trace_stamp(a, q, 2);
+      mbar_arrive(&S.sempty[q % kSSlots]);
+    }
+    return stop;
+  };
+
+  Carry cur = stress_tile(0);
+  if (stress_done(0)) return;
+  for (int q = 0; q < nq; q++) {
+    stepu_tile(q, cur);
+    if (q + 1 >= nq) break;
+    const Carry nxt = stress_tile(q + 1);
+    if (stress_done(q + 1)) break;
+    cur = nxt;
   }
 }
 
@@ -586,6 +765,14 @@ __global__ void k_wait_probe(int *err, unsigned long long limit_ns) {
   }
 }
 
+// The same for the dependency wait of a multi-subcycle launch: one thread
+// waits on a counter that nothing raises.
+constexpr int kDepProbeCode = 14;
+
+__global__ void k_dep_probe(int *err, const unsigned *counter, unsigned long long limit_ns) {
+  if (threadIdx.x == 0) wait_counter(counter, 1u, err, kDepProbeCode, limit_ns);
+}
+
 }  // namespace
 
 const char *tma_wait_name(int code) {
@@ -596,17 +783,19 @@ const char *tma_wait_name(int code) {
     case 6: return "the producer waited for a tile record";
     case 7: return "the producer waited for records issued ahead";
     case 8: return "the dynamic shared memory was not 16-byte aligned";
-    case 9: return "the producer waited for the stepu slot";
-    case 10: return "the producer waited for its last stepu copy";
+    case 9: return "the stepu-part warp waited for the stepu slot";
+    case 10: return "the stepu-part warp waited for its last copy";
     case 11: return "a consumer waited for a tile's stepu inputs";
+    case 13: return "the producer waited for neighbouring tiles to finish a subcycle";
     case kProbeCode: return "the wait probe (evp1d_debug_wait_timeout)";
+    case kDepProbeCode: return "the dependency-wait probe (evp1d_debug_dep_wait_timeout)";
     default: return "unknown";
   }
 }
 
 cudaError_t tma_binary_version(int *version) {
   cudaFuncAttributes at;
-  const cudaError_t e = cudaFuncGetAttributes(&at, k_tma<false, true>);
+  const cudaError_t e = cudaFuncGetAttributes(&at, k_tma<false, true, false>);
   if (e == cudaSuccess) *version = at.binaryVersion;
   return e;
 }
@@ -615,29 +804,55 @@ void launch_wait_probe(int *err, unsigned long long limit_ns, cudaStream_t st) {
   k_wait_probe<<<1, 32, 0, st>>>(err, limit_ns);
 }
 
+void launch_dep_probe(int *err, const unsigned *counter, unsigned long long limit_ns,
+                      cudaStream_t st) {
+  k_dep_probe<<<1, 32, 0, st>>>(err, counter, limit_ns);
+}
+
+using TmaKernel = void (*)(TmaArgs, Params);
+constexpr int kTmaKernels = 6;
+const TmaKernel kTmaAll[kTmaKernels] = {
+    k_tma<false, false, false>, k_tma<true, false, false>, k_tma<false, true, false>,
+    k_tma<true, true, false>,   k_tma<false, false, true>, k_tma<false, true, true>};
+
 int tma_prepare(int device) {
   const int bytes = (int)smem_bytes();
-  void (*const ks[4])(TmaArgs, Params) = {k_tma<false, false>, k_tma<true, false>,
-                                          k_tma<false, true>, k_tma<true, true>};
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < 4 && e == cudaSuccess; i++)
-    e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  for (int i = 0; i < kTmaKernels && e == cudaSuccess; i++)
+    e = cudaFuncSetAttribute(kTmaAll[i], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   (void)device;
   return e == cudaSuccess ? 0 : (int)e;
 }
 
-void launch_tma(const TmaArgs &a, const Params &p, bool last, cudaStream_t st) {
-  if (a.ntiles <= 0 || a.nruns <= 0) return;
-  const int grid = a.nruns;
+bool tma_can_persist(int device, int nruns) {
+  int coop = 0, sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tma<false, true, true>, kThreads,
+                                                    smem_bytes()) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return coop != 0 && nruns <= sms * per_sm;
+}
+
+cudaError_t launch_tma(const TmaArgs &a, const Params &p, cudaStream_t st) {
+  if (a.ntiles <= 0 || a.nruns <= 0 || a.nsub <= 0) return cudaSuccess;
   const bool std = std_params(p);
-  if (last && std)
-    k_tma<true, true><<<grid, kThreads, smem_bytes(), st>>>(a, p);
-  else if (last)
-    k_tma<true, false><<<grid, kThreads, smem_bytes(), st>>>(a, p);
-  else if (std)
-    k_tma<false, true><<<grid, kThreads, smem_bytes(), st>>>(a, p);
-  else
-    k_tma<false, false><<<grid, kThreads, smem_bytes(), st>>>(a, p);
+  if (a.nsub > 1 && a.epoch) {
+    // CTAs wait on one another: all of them resident at once
+    TmaKernel k = std ? k_tma<false, true, true> : k_tma<false, false, true>;
+    TmaArgs aa = a;
+    Params pp = p;
+    void *args[] = {&aa, &pp};
+    return cudaLaunchCooperativeKernel((const void *)k, dim3(a.nruns), dim3(kThreads), args,
+                                       smem_bytes(), st);
+  }
+  if (a.nsub != 1) return cudaErrorInvalidValue;  // several subcycles need the counters
+  TmaKernel k = a.last ? (std ? k_tma<true, true, false> : k_tma<true, false, false>)
+                       : (std ? k_tma<false, true, false> : k_tma<false, false, false>);
+  k<<<a.nruns, kThreads, smem_bytes(), st>>>(a, p);
+  return cudaGetLastError();
 }
 
 }  // namespace evp

@@ -264,6 +264,33 @@ long long verify_tile_plan(const TilePlan &P, const int32_t *const nb0[6], int m
       if (s >= 0 && s < nuv) xpos[s] = -1;
     }
   }
+  if (bad) return bad;
+
+  // subcycle dependencies: exactly the owners of what each tile reads (its
+  // own points, extras and halo) and the tiles that read its points
+  if (P.dep_off.size() != (size_t)T + 1 || P.dep_off.front() != 0 ||
+      (size_t)P.dep_off.back() != P.dep_idx.size()) {
+    note(bad, first, "dependency lists: %zu offsets for %d tiles", P.dep_off.size(), T);
+    return bad;
+  }
+  std::vector<std::vector<int32_t>> want((size_t)T);
+  for (int t = 0; t < T; t++) {
+    want[t].push_back(t);
+    for (int x = P.uvx_off[t]; x < P.uvx_off[t] + P.uvx_cnt[t]; x++)
+      if (P.uvx_idx[x] < S) want[t].push_back(tile_of[P.uvx_idx[x]]);
+    for (int h = P.halo_off[t]; h < P.halo_off[t] + P.halo_cnt[t]; h++)
+      want[t].push_back(tile_of[P.halo_idx[h]]);
+  }
+  for (int t = 0; t < T; t++)
+    for (size_t k = 0, n = want[t].size(); k < n; k++) want[want[t][k]].push_back(t);
+  for (int t = 0; t < T; t++) {
+    std::sort(want[t].begin(), want[t].end());
+    want[t].erase(std::unique(want[t].begin(), want[t].end()), want[t].end());
+    const int d0 = P.dep_off[t], d1 = P.dep_off[t + 1];
+    if (d1 < d0 || (size_t)(d1 - d0) != want[t].size() ||
+        !std::equal(want[t].begin(), want[t].end(), P.dep_idx.begin() + d0))
+      note(bad, first, "tile %d: %d dependencies, want %zu", t, d1 - d0, want[t].size());
+  }
   return bad;
 }
 

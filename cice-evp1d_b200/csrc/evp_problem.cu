@@ -50,7 +50,8 @@ int d2h(void *dst, const void *src, size_t bytes, cudaStream_t st) {
   return EVP1D_OK;
 }
 
-void layout(DeviceProblem *d, Carve &c, size_t nhalo_total, size_t nuvx_total) {
+void layout(DeviceProblem *d, Carve &c, size_t nhalo_total, size_t nuvx_total,
+            size_t ndep_total) {
   const size_t S = (size_t)d->nslots, U = (size_t)d->nuv, T = (size_t)d->ntiles;
   c.take(&d->err, 1);
   c.take(&d->meta, S);
@@ -64,6 +65,9 @@ void layout(DeviceProblem *d, Carve &c, size_t nhalo_total, size_t nuvx_total) {
   c.take(&d->tile_rec, (size_t)kRecInts * T);
   c.take(&d->cblk, (size_t)kConstFields * kConstTileSlots * T);
   c.take(&d->run_off, (size_t)d->nruns + 1);
+  c.take(&d->dep_off, T + 1);
+  c.take(&d->dep_idx, ndep_total);
+  c.take(&d->epoch, T);
   c.take(&d->tile_off, T);
   c.take(&d->tile_cnt, T);
   c.take(&d->halo_off, T);
@@ -107,12 +111,12 @@ int problem_create(DeviceProblem *d, int device, const TilePlan &plan,
   if (tma_prepare(device) != 0)
     return error(EVP1D_ERR_CUDA, "cannot enable %d bytes of shared memory", 0);
   Carve sizing;
-  layout(d, sizing, plan.halo_idx.size(), plan.uvx_idx.size());
+  layout(d, sizing, plan.halo_idx.size(), plan.uvx_idx.size(), plan.dep_idx.size());
   CUDA_TRY(device_alloc(&d->arena, sizing.off));
   d->arena_bytes = sizing.off;
   Carve c;
   c.base = (char *)d->arena;
-  layout(d, c, plan.halo_idx.size(), plan.uvx_idx.size());
+  layout(d, c, plan.halo_idx.size(), plan.uvx_idx.size(), plan.dep_idx.size());
   cudaStream_t st = d->stream;
   CUDA_TRY(cudaMemsetAsync(d->arena, 0, d->arena_bytes, st));
   if (d->na == 0) {
@@ -122,6 +126,8 @@ int problem_create(DeviceProblem *d, int device, const TilePlan &plan,
   const size_t T = (size_t)d->ntiles * sizeof(int32_t);
   const size_t S4 = (size_t)d->nslots * sizeof(int32_t);
   TRY(h2d(d->run_off, plan.run_off.data(), plan.run_off.size() * sizeof(int32_t), st));
+  TRY(h2d(d->dep_off, plan.dep_off.data(), plan.dep_off.size() * sizeof(int32_t), st));
+  TRY(h2d(d->dep_idx, plan.dep_idx.data(), plan.dep_idx.size() * sizeof(int32_t), st));
   TRY(h2d(d->tile_off, plan.tile_off.data(), T, st));
   TRY(h2d(d->tile_cnt, plan.tile_cnt.data(), T, st));
   TRY(h2d(d->halo_off, plan.halo_off.data(), T, st));
@@ -476,19 +482,23 @@ TmaArgs problem_tma_args(const DeviceProblem &d, int from) {
   a.tile_meta = d.tile_meta;
   a.tile_rec = d.tile_rec;
   const int geo_order[6] = {kDxT, kDyT, kHTE, kHTN, kHTEm1, kHTNm1};
-  for (int k = 0; k < 6; k++) a.sf[k] = d.geo[geo_order[k]];
-  a.sf[6] = d.dyn[kStrength];
-  for (int k = 0; k < 12; k++) a.sf[7 + k] = d.stress[from][k];
+  for (int k = 0; k < 6; k++) a.sg[k] = d.geo[geo_order[k]];
+  a.sg[6] = d.dyn[kStrength];
   a.cblk = d.cblk;
-  a.u_in = d.u[from];
-  a.v_in = d.v[from];
-  a.u_out = d.u[to];
-  a.v_out = d.v[to];
-  for (int k = 0; k < 12; k++) a.s_out[k] = d.stress[to][k];
+  a.u[0] = d.u[from];
+  a.v[0] = d.v[from];
+  a.u[1] = d.u[to];
+  a.v[1] = d.v[to];
+  for (int k = 0; k < 12; k++) {
+    a.s[0][k] = d.stress[from][k];
+    a.s[1][k] = d.stress[to][k];
+  }
   a.strintx = d.strintx;
   a.strinty = d.strinty;
   a.Cb = d.Cb;
   for (int k = 0; k < 8; k++) a.str_out[k] = d.str[k];
+  a.dep_off = d.dep_off;
+  a.dep_idx = d.dep_idx;
   a.err = d.err;
   return a;
 }

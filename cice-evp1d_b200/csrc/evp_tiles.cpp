@@ -274,6 +274,7 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
   P.navel = navel;
   P.nhalo_slots = navel - na;
   P.run_off.assign(1, 0);
+  P.dep_off.assign(1, 0);
   if (na == 0) return;
 
   // ---- steps 1 + 2: the order ----------------------------------------------
@@ -427,6 +428,35 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
       ppos[q] = own + h;
     }
   }
+
+  // ---- subcycle-to-subcycle dependencies ------------------------------------
+  // reads[t]: owners of the list points tile t reads; deps = reads + reverse
+  std::vector<std::vector<int32_t>> deps((size_t)P.ntiles);
+  for (int t = 0; t < P.ntiles; t++) {
+    std::vector<int32_t> &r = deps[t];
+    r.push_back(t);
+    for (int x = P.uvx_off[t]; x < P.uvx_off[t] + P.uvx_cnt[t]; x++)
+      if (P.uvx_idx[x] < P.nslots) r.push_back(tile_of[P.point_of_slot[P.uvx_idx[x]]]);
+    for (int h = P.halo_off[t]; h < P.halo_off[t] + P.halo_cnt[t]; h++)
+      r.push_back(tile_of[P.point_of_slot[P.halo_idx[h]]]);
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+  }
+  for (int t = 0; t < P.ntiles; t++)
+    for (size_t k = 0; k < deps[t].size(); k++) {
+      const int u = deps[t][k];
+      if (u != t && u >= 0 && !std::binary_search(deps[u].begin(), deps[u].end(), t))
+        deps[u].push_back(t);  // sorted again below
+    }
+  P.dep_off.assign((size_t)P.ntiles + 1, 0);
+  for (int t = 0; t < P.ntiles; t++) {
+    std::sort(deps[t].begin(), deps[t].end());
+    deps[t].erase(std::unique(deps[t].begin(), deps[t].end()), deps[t].end());
+    P.dep_off[t + 1] = P.dep_off[t] + (int)deps[t].size();
+  }
+  P.dep_idx.reserve((size_t)P.dep_off[P.ntiles]);
+  for (int t = 0; t < P.ntiles; t++)
+    P.dep_idx.insert(P.dep_idx.end(), deps[t].begin(), deps[t].end());
 }
 
 }  // namespace evp

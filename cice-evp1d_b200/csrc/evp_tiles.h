@@ -77,6 +77,11 @@ struct TilePlan {
   // extra velocity points of each tile (u/v slots outside its owned range)
   std::vector<int32_t> uvx_off, uvx_cnt;  // [ntiles]
   std::vector<int32_t> uvx_idx;
+  // tiles a tile depends on from one subcycle to the next: the owners of
+  // every point it reads (itself, its extras, its forward halo) and the
+  // tiles that read any of its points; sorted, CSR [dep_off[t], dep_off[t+1])
+  std::vector<int32_t> dep_off;  // [ntiles + 1]
+  std::vector<int32_t> dep_idx;
 };
 
 // Build the plan from 0-based neighbour vectors (values in [0, navel)) for a

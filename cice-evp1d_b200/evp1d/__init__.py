@@ -427,6 +427,13 @@ class EVP1D:
         (evp1d_debug_wait_timeout): the next synchronize raises the timeout."""
         check(self._L.evp1d_debug_wait_timeout(self.h, int(ns)), "evp1d_debug_wait_timeout")
 
+    def debug_dep_wait_timeout(self, ns: int) -> None:
+        """Queue one bounded wait of the multi-subcycle launch's kind, on a
+        counter nothing raises (evp1d_debug_dep_wait_timeout): the next
+        synchronize raises the timeout."""
+        check(self._L.evp1d_debug_dep_wait_timeout(self.h, int(ns)),
+              "evp1d_debug_dep_wait_timeout")
+
     @property
     def path(self) -> str:
         """Name of the kernel path the library runs."""

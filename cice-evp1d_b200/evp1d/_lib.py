@@ -111,6 +111,8 @@ def load() -> C.CDLL:
     L.evp1d_debug_trace.restype = C.c_int
     L.evp1d_debug_wait_timeout.argtypes = [H, C.c_longlong]
     L.evp1d_debug_wait_timeout.restype = C.c_int
+    L.evp1d_debug_dep_wait_timeout.argtypes = [H, C.c_longlong]
+    L.evp1d_debug_dep_wait_timeout.restype = C.c_int
     L.evp1d_kernel_path.argtypes = [H]
     L.evp1d_kernel_path.restype = C.c_char_p
     L.evp1d_build_index.argtypes = ([C.c_int, C.c_int, C.c_int, _I, C.c_int,

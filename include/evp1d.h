@@ -170,6 +170,15 @@ int evp1d_synchronize(evp1d_t *handle);
  * and clears it; the handle stays usable. */
 int evp1d_debug_wait_timeout(evp1d_t *handle, long long ns);
 
+/* Debug: the same for the other bounded wait of the solver.  A call's
+ * subcycles run in one launch whose CTAs stay resident; before a tile loads
+ * the next subcycle's state, its CTA waits on per-tile counters until the
+ * tiles it depends on have finished the subcycle before.  This queues one
+ * such wait on a counter that nothing raises, limited to `ns` nanoseconds
+ * (1e6 to 1e9); it runs out, and the next check returns EVP1D_ERR_TIMEOUT
+ * naming it.  No counterpart in the reference. */
+int evp1d_debug_dep_wait_timeout(evp1d_t *handle, long long ns);
+
 /* Debug: host-side injection of an out-of-memory failure.  The n-th device
  * allocation of the library after this call (1 = the next one) fails as if
  * the device were full: it allocates nothing, and the call that made it

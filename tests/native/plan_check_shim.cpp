@@ -72,6 +72,15 @@ bool plant(evp::TilePlan &P, int kind) {
       }
       return false;
     }
+    case 17: {  // a dependency dropped
+      for (int u = 0; u < P.ntiles; u++)
+        if (P.dep_off[u + 1] - P.dep_off[u] > 1) {
+          P.dep_idx.erase(P.dep_idx.begin() + P.dep_off[u]);
+          for (int v = u + 1; v <= P.ntiles; v++) P.dep_off[v]--;
+          return true;
+        }
+      return false;
+    }
     default: return false;
   }
 }
@@ -80,7 +89,7 @@ bool plant(evp::TilePlan &P, int kind) {
 
 extern "C" {
 
-int shim_kinds(void) { return 16; }
+int shim_kinds(void) { return 17; }
 
 // 1-based neighbour vectors as evp1d_init takes them.  Returns the number of
 // violations found (0 for kind 0 on a good plan), or -1 if the mistake could

@@ -344,3 +344,26 @@ def test_adjoint_general_parameters_match_tape(oracle_mod):
         assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
     assert rel(g["uvel"], t["uvel0"]) < 1e-9
     assert rel(g["stress"], t["stress0"]) < 1e-9
+
+
+@pytest.mark.parametrize("interval,persist", [(0, "0"), (3, "0"), (3, "1")])
+def test_adjoint800x600_grid_matches_tape(oracle_mod, monkeypatch, interval, persist):
+    """The adjoint benchmark's own grid (800 x 600, 294,541 points) at a
+    reduced ndte, against the taped FP64 restatement: the gradients the bench
+    differentiates are the tape's to 1e-9, so its finite-difference residuals
+    are finite-difference error, not adjoint error.  interval = 3 recomputes
+    checkpointed segments of three subcycles; with EVP1D_PERSIST=1 each
+    segment, and the taped tail, is one multi-subcycle launch writing a tape
+    entry per subcycle."""
+    import evp_tape
+    monkeypatch.setenv("EVP1D_PERSIST", persist)
+    ndte = 7
+    pr = synth.make_problem("adjoint800x600", ndte=ndte)
+    assert pr.na > 250_000
+    uobs, vobs = synth.observations(pr.na, seed=synth.CONFIGS["adjoint800x600"]["seed"] + 500)
+    p = evp1d.set_evp_parameters(ndte)
+    g, fs, info = gpu_grads(pr, ndte, uobs, vobs, interval=interval)
+    assert info["valid"] == 1
+    t = evp_tape.gradient(pr, ndte, p, uobs, vobs)
+    for k in FIELDS:
+        assert rel(g[k], t[k]) < 1e-9, (k, rel(g[k], t[k]))
