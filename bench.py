@@ -630,7 +630,7 @@ def run_split(args, rank, world, local):
 
     MAX = pg.ReduceOp.MAX if pg else None
     SUM = pg.ReduceOp.SUM if pg else None
-    s.upload(evp1d.FieldSet.from_problem(band.local))
+    bsol.upload(evp1d.FieldSet.from_problem(band.local))
     for _ in range(args.warmup):
         sweep(ndte)
     s.synchronize()
@@ -644,12 +644,14 @@ def run_split(args, rank, world, local):
     if sampler:
         sampler.__enter__()
     s.launch_count(reset=True)
+    bsol.graph_launches = 0
     e0.record(stream)
     for _ in range(args.steps):
         sweep(ndte)
     e1.record(stream)
     e1.synchronize()
-    launches = s.launch_count()
+    # kernels issued directly plus those the band's CUDA graphs replayed
+    launches = s.launch_count() + bsol.graph_launches
     if sampler:
         sampler.__exit__(None, None, None)
     t_dev = e0.elapsed_time(e1) / 1000.0
@@ -922,6 +924,27 @@ def run_band_timing(args, local):
                 out["ring"].append(b.local.na - b.n_own)
                 out["send_bytes"].append(16 * len(b.send_idx()))
         out["max_us"] = max(out["us"])
+        if nb == 1:
+            # the same one-band step through BandSolver (graphs of 50 steps)
+            # against evp1d_subcycles of the band's problem
+            b = bands.split(pr, 1)[0]
+            with bands.BandSolver(b, device=local) as bsol:
+                bsol.upload(evp1d.FieldSet.from_problem(b.local))
+                stream = torch.cuda.ExternalStream(bsol.s.stream, device=dev)
+                bsol.subcycles(100)
+                bsol.s.synchronize()
+                e0, e1 = _event_pair()
+                e0.record(stream)
+                bsol.subcycles(nsub)
+                e1.record(stream)
+                e1.synchronize()
+                out["band_solver_graphed_us"] = 1000.0 * e0.elapsed_time(e1) / nsub
+                e0, e1 = _event_pair()
+                e0.record(stream)
+                bsol.s.subcycles(nsub)
+                e1.record(stream)
+                e1.synchronize()
+                out["evp1d_subcycles_us"] = 1000.0 * e0.elapsed_time(e1) / nsub
         print(json.dumps(out), flush=True)
 
 

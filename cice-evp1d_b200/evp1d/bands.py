@@ -209,6 +209,8 @@ class BandSolver:
         self.band, self.group = band, group
         self.device = torch.device("cuda", device)
         self.s = EVP1D.from_problem(band.local, ndte=ndte, params=params, device=device)
+        self._graphs, self._parity = {}, 0
+        self._graph_delta, self.graph_launches = 0, 0
         self.s.exchange_setup(band.send_idx(), band.recv_idx())
         ps, pr = self.s.exchange_buffers()
         self.send_buf = device_view(ps, 2 * len(band.send_idx()), self.device)
@@ -219,22 +221,59 @@ class BandSolver:
             # point-to-point operation later
             dist.barrier(group=group)
 
+    #: steps per captured CUDA graph (even: a graph leaves the ping-pong
+    #: parity where it found it); 0 runs every step eagerly
+    GRAPH_STEPS = 50
+
+    def _steps(self, n: int) -> None:
+        s = self.s
+        run_band(self.band, n, lambda: s.subcycles(1), lambda b: s.exchange_pack(),
+                 lambda b: s.exchange_unpack(), self.send_buf, self.recv_buf, self.group)
+
     def subcycles(self, n: int) -> None:
         """`n` subcycles of the uploaded band, each followed by the exchange,
-        all ordered on the handle's stream."""
+        all ordered on the handle's stream.  Whole chunks of GRAPH_STEPS steps
+        (subcycle, pack, the NCCL send/recv, unpack) are captured once per
+        ping-pong parity into a CUDA graph and replayed; the rest runs
+        eagerly.  Kernels replayed this way are counted in graph_launches."""
         import torch
         s = self.s
-        with torch.cuda.stream(torch.cuda.ExternalStream(s.stream, device=self.device)):
-            run_band(self.band, n, lambda: s.subcycles(1), lambda b: s.exchange_pack(),
-                     lambda b: s.exchange_unpack(), self.send_buf, self.recv_buf, self.group)
+        stream = torch.cuda.ExternalStream(s.stream, device=self.device)
+        G = self.GRAPH_STEPS
+        with torch.cuda.stream(stream):
+            while G > 0 and n >= G and self._graphs is not False:
+                g = self._graphs.get(self._parity)
+                if g is None:
+                    before = s.launch_count()
+                    g = torch.cuda.CUDAGraph()
+                    try:
+                        with torch.cuda.graph(g, stream=stream):
+                            self._steps(G)
+                    except Exception:
+                        # a transport that cannot be captured runs eagerly
+                        self._graphs = False
+                        break
+                    self._graph_delta = s.launch_count() - before
+                    self._graphs[self._parity] = g
+                g.replay()
+                self.graph_launches += self._graph_delta
+                n -= G
+            self._steps(n)
+        self._parity ^= n & 1
+
+    def upload(self, fields) -> None:
+        self.s.upload(fields)
+        self._parity = 0  # the library starts every upload from set 0
 
     def run(self, ndte: int, fields):
-        self.s.upload(fields)
+        self.upload(fields)
         self.subcycles(ndte)
         self.s.download(fields)
         return fields
 
     def finalize(self) -> None:
+        # graphs that hold NCCL operations go before the communicator
+        self._graphs = {}
         self.s.finalize()
 
     def __enter__(self):

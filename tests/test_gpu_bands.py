@@ -99,6 +99,27 @@ def test_band_solver_world_size_one(oracle_mod):
     _same(B.assemble(pr, [band], [_outs(fs)]), oracle_run(oracle_mod, pr, 9), pr)
 
 
+@pytest.mark.parametrize("graph_steps", [0, 4])
+def test_band_solver_graphs_bitwise(oracle_mod, monkeypatch, graph_steps):
+    """The band step captured in CUDA graphs of 4 steps (and, for
+    comparison, eagerly): 11 and then 11 more subcycles of one upload, so
+    that graphs are captured for both ping-pong parities and replayed, with
+    eager steps between them.  Bit for bit the oracle's 22 subcycles."""
+    monkeypatch.setattr(B.BandSolver, "GRAPH_STEPS", graph_steps)
+    pr = synth.make_problem("grid400x300", nx=100, ny=80, ndte=22)
+    band = B.split(pr, 1)[0]
+    fs = evp1d.FieldSet.from_problem(band.local)
+    with B.BandSolver(band, ndte=22) as bsol:
+        bsol.upload(fs)
+        bsol.subcycles(11)
+        bsol.subcycles(11)
+        bsol.s.download(fs)
+        if graph_steps:
+            assert bsol.graph_launches > 0
+            assert set(bsol._graphs) == {0, 1}
+    _same(B.assemble(pr, [band], [_outs(fs)]), oracle_run(oracle_mod, pr, 22), pr)
+
+
 def test_exchange_setup_validation():
     pr = synth.to_1d(synth.make_grid(40, 30, seed=2, ndte=4))
     with evp1d.EVP1D.from_problem(pr, ndte=4) as s:
