@@ -236,13 +236,14 @@ int check_device(int device) {
 // on (evp1d_set_tile_points).
 std::atomic<int> g_tile_points{evp::kTileCompute};
 
-// Strip width of the grid order: EVP1D_STRIP_W (1..128), else the default.
+// Strip width of the grid order: EVP1D_STRIP_W (1..128), else 0 (the planner
+// chooses by the points per run).
 int strip_width() {
   if (const char *e = getenv("EVP1D_STRIP_W")) {
     const int v = atoi(e);
     if (v >= 1 && v <= 128) return v;
   }
-  return evp::kStripWidth;
+  return 0;
 }
 
 // Runs (CTAs) of the plans made without a device: the B200's SM count.
@@ -495,8 +496,12 @@ int evp1d_upload(evp1d_t *h, const evp1d_fields *io) {
   return EVP1D_OK;
 }
 
-int evp1d_subcycles(evp1d_t *h, int ndte) {
-  evp::NvtxRange nvtx_range("evp1d_subcycles");
+}  // extern "C"
+
+namespace {
+// ndte subcycles; `ends` = the last one ends the call (writes strintx,
+// strinty, Cb and str).
+int run_subcycles(evp1d_t *h, int ndte, bool ends) {
   if (!h) return fail(EVP1D_ERR_INVALID_ARG, "NULL handle");
   if (ndte < 0) return fail(EVP1D_ERR_INVALID_ARG, "ndte = %d < 0", ndte);
   if (!h->uploaded) return fail(EVP1D_ERR_STATE, "evp1d_upload has not been called");
@@ -509,7 +514,7 @@ int evp1d_subcycles(evp1d_t *h, int ndte) {
     evp::TmaArgs a = evp::problem_tma_args(h->d, h->d.cur);
     a.trace = h->trace;
     a.nsub = ndte;
-    a.last = true;
+    a.last = ends;
     a.epoch = h->d.epoch;
     CUDA_TRY(evp::launch_tma(a, h->p, st));
     if (ndte & 1) h->d.cur = 1 - h->d.cur;
@@ -529,11 +534,24 @@ int evp1d_subcycles(evp1d_t *h, int ndte) {
     h->d.cur = 1 - h->d.cur;
     h->launches++;
   }
-  launch_sub(h, h->d.cur, true);
+  launch_sub(h, h->d.cur, ends);
   h->d.cur = 1 - h->d.cur;
   h->launches++;
   CUDA_TRY(cudaGetLastError());
   return EVP1D_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int evp1d_subcycles(evp1d_t *h, int ndte) {
+  evp::NvtxRange nvtx_range("evp1d_subcycles");
+  return run_subcycles(h, ndte, true);
+}
+
+int evp1d_subcycles_inner(evp1d_t *h, int n) {
+  evp::NvtxRange nvtx_range("evp1d_subcycles_inner");
+  return run_subcycles(h, n, false);
 }
 
 int evp1d_download(evp1d_t *h, const evp1d_fields *io) {

@@ -267,7 +267,9 @@ void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
                      TilePlan *plan, int max_tile, int nruns, int strip_w) {
   const int tmax = max_tile < 1 ? 1 : (max_tile > kTileCompute ? kTileCompute : max_tile);
   const int want_runs = nruns < 1 ? 1 : nruns;
-  const int w = strip_w < 1 ? 1 : strip_w;
+  const int w = strip_w >= 1 ? strip_w
+                             : ((long long)na >= (long long)kStripWideRun * want_runs ? kStripWide
+                                                                                     : kStripNarrow);
   TilePlan &P = *plan;
   P = TilePlan();
   P.na = na;

@@ -50,8 +50,14 @@ constexpr int kRecInts = kRecHLcc + kTileHalo;
 constexpr int kSlotAlign = 4;     // tile starts are multiples of 4 slots (32 B)
 constexpr int kLnbBits = 10;      // bits per packed local index
 constexpr uint32_t kLnbMask = (1u << kLnbBits) - 1;
-// Default width (grid columns) of the strips the grid points are ordered in.
-constexpr int kStripWidth = 48;
+// Widths (grid columns) of the strips the grid points are ordered in, chosen
+// by the points per run: wide strips recompute less of the strip's right
+// edge, narrow ones less of the row above a run's first tile, which matters
+// when runs are short (grid1600x1200, 8,000 points per run: 97.9 us per
+// subcycle at 64 columns against 100.1 at 48 and 100.3 at 80; the halo cap
+// of 64 points bounds the width).
+constexpr int kStripWide = 64, kStripNarrow = 48;
+constexpr int kStripWideRun = 4096;  // points per run from which strips are wide
 
 struct TilePlan {
   int na = 0, navel = 0;
@@ -89,11 +95,11 @@ struct TilePlan {
 // are reconstructed from the neighbour graph, and if that is inconsistent
 // the points keep their list order.  A tile's compute set (owned points plus
 // forward halo) holds at most max_tile points (1..kTileCompute); strip_w is
-// the width of the strips grid points are ordered in.
+// the width of the strips grid points are ordered in (0: by points per run).
 void build_tile_plan(int na, int navel, const int32_t *const nb0[6],
                      const int32_t *coords_i, const int32_t *coords_j,
                      TilePlan *plan, int max_tile = kTileCompute, int nruns = 148,
-                     int strip_w = kStripWidth);
+                     int strip_w = 0);
 
 // Decode every index of `plan` that the kernels gather through (slot maps,
 // runs and tile ranges, neighbour slots, forward halos, velocity extras, the

@@ -334,6 +334,11 @@ class EVP1D:
     def subcycles(self, ndte: int) -> None:
         check(self._L.evp1d_subcycles(self.h, int(ndte)), "evp1d_subcycles")
 
+    def subcycles_inner(self, n: int) -> None:
+        """Subcycles that do not end the call (evp1d_subcycles_inner): the
+        state advances, strintx/strinty/Cb/str are not written."""
+        check(self._L.evp1d_subcycles_inner(self.h, int(n)), "evp1d_subcycles_inner")
+
     def download(self, fields: FieldSet) -> FieldSet:
         check(self._L.evp1d_download(self.h, C.byref(fields.c)), "evp1d_download")
         return fields

@@ -89,6 +89,7 @@ def load() -> C.CDLL:
     L.evp1d_run.argtypes = [H, C.c_int, C.POINTER(Fields)]
     L.evp1d_upload.argtypes = [H, C.POINTER(Fields)]
     L.evp1d_subcycles.argtypes = [H, C.c_int]
+    L.evp1d_subcycles_inner.argtypes = [H, C.c_int]
     L.evp1d_download.argtypes = [H, C.POINTER(Fields)]
     L.evp1d_stress_only.argtypes = [H, C.c_int]
     L.evp1d_stepu_only.argtypes = [H, C.c_int]

@@ -225,23 +225,36 @@ class BandSolver:
     #: parity where it found it); 0 runs every step eagerly
     GRAPH_STEPS = 50
 
-    def _steps(self, n: int) -> None:
+    def _steps(self, n: int, ends: bool = False) -> None:
+        """n band steps; with `ends`, the last one's subcycle ends the call
+        (writes strintx, strinty, Cb and str), the others do not."""
         s = self.s
-        run_band(self.band, n, lambda: s.subcycles(1), lambda b: s.exchange_pack(),
+        if n <= 0:
+            return
+        if ends:
+            if n > 1:
+                self._steps(n - 1)
+            run_band(self.band, 1, lambda: s.subcycles(1), lambda b: s.exchange_pack(),
+                     lambda b: s.exchange_unpack(), self.send_buf, self.recv_buf, self.group)
+            return
+        run_band(self.band, n, lambda: s.subcycles_inner(1), lambda b: s.exchange_pack(),
                  lambda b: s.exchange_unpack(), self.send_buf, self.recv_buf, self.group)
 
     def subcycles(self, n: int) -> None:
         """`n` subcycles of the uploaded band, each followed by the exchange,
-        all ordered on the handle's stream.  Whole chunks of GRAPH_STEPS steps
-        (subcycle, pack, the NCCL send/recv, unpack) are captured once per
-        ping-pong parity into a CUDA graph and replayed; the rest runs
-        eagerly.  Kernels replayed this way are counted in graph_launches."""
+        all ordered on the handle's stream, the last one ending the call.
+        Whole chunks of GRAPH_STEPS steps (subcycle, pack, the NCCL
+        send/recv, unpack) are captured once per ping-pong parity into a CUDA
+        graph and replayed; the rest runs eagerly.  Kernels replayed this way
+        are counted in graph_launches."""
         import torch
         s = self.s
         stream = torch.cuda.ExternalStream(s.stream, device=self.device)
         G = self.GRAPH_STEPS
         with torch.cuda.stream(stream):
-            while G > 0 and n >= G and self._graphs is not False:
+            # whole graphs, then the rest eagerly, the very last subcycle
+            # ending the call
+            while G > 0 and n > G and self._graphs is not False:
                 g = self._graphs.get(self._parity)
                 if g is None:
                     before = s.launch_count()
@@ -258,7 +271,7 @@ class BandSolver:
                 g.replay()
                 self.graph_launches += self._graph_delta
                 n -= G
-            self._steps(n)
+            self._steps(n, ends=True)
         self._parity ^= n & 1
 
     def upload(self, fields) -> None:

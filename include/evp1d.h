@@ -149,7 +149,13 @@ int evp1d_run(evp1d_t *handle, int ndte, const evp1d_fields *io);
 /* The same call split in three, for callers that keep the state on the GPU
  * between calls or time the device work alone. */
 int evp1d_upload(evp1d_t *handle, const evp1d_fields *io);
-int evp1d_subcycles(evp1d_t *handle, int ndte); /* device-resident */
+int evp1d_subcycles(evp1d_t *handle, int ndte);
+/* Subcycles that do not end a call: the same state update, without the
+ * outputs the last subcycle of a call writes (strintx, strinty, Cb,
+ * str1..str8).  For a caller that interleaves its own work between
+ * subcycles (the velocity exchange of a split state) and ends the call with
+ * evp1d_subcycles.  No counterpart in the reference. */
+int evp1d_subcycles_inner(evp1d_t *handle, int n); /* device-resident */
 int evp1d_download(evp1d_t *handle, const evp1d_fields *io);
 
 /* lindividual-style loops on the device-resident state
