@@ -394,6 +394,9 @@ def run_adjoint(args, rank, world, local):
     for _ in range(args.warmup):
         s.subcycles(ndte)
         _adjoint_once(s, stream, ndte, interval, lam, fields)
+        # the memory-sized recording too: its larger store is allocated here,
+        # not in the timed steps
+        _adjoint_once(s, stream, ndte, 0, lam, fields)
     s.upload(fields())
     props = torch.cuda.get_device_properties(local)
     gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
@@ -885,9 +888,11 @@ def run_band_timing(args, local):
     """--band-timing K...: the per-rank work of a split of --config into K
     bands, measured on one GPU.  Each band's handle runs 200 steps of (one
     subcycle, pack, unpack) on its own stream, timed with CUDA events on that
-    stream; the exchange between GPUs (NCCL) is not part of it.  One JSON line
-    per K: microseconds per step of every band and the bytes each band sends
-    per subcycle."""
+    stream; the exchange between GPUs (NCCL) is not part of it.  `us`: every
+    step launched on its own and ending a call; `graphed_us`: the steps
+    replayed from CUDA graphs of GRAPH_STEPS steps that do not end the call,
+    as BandSolver runs them.  One JSON line per K: microseconds per step of
+    every band and the bytes each band sends per subcycle."""
     import torch
     import evp1d
     from evp1d import synth, bands
@@ -896,17 +901,21 @@ def run_band_timing(args, local):
     dev = torch.device("cuda", local)
     pr = synth.make_problem(args.config)
     nsub, warmup = 200, 5
+    G = bands.BandSolver.GRAPH_STEPS
     for nb in (args.band_timing or [1, 2, 4, 8]):
-        out = dict(problem=args.config, na=pr.na, nbands=nb, us=[], points=[], ring=[],
-                   send_bytes=[])
+        out = dict(problem=args.config, na=pr.na, nbands=nb, us=[], graphed_us=[], points=[],
+                   ring=[], send_bytes=[])
         for b in bands.split(pr, nb):
             with evp1d.EVP1D.from_problem(b.local, device=local) as s:
                 s.exchange_setup(b.send_idx(), b.recv_idx())
                 s.upload(evp1d.FieldSet.from_problem(b.local))
                 stream = torch.cuda.ExternalStream(s.stream, device=dev)
 
-                def step():
-                    s.subcycles(1)
+                def step(inner=False):
+                    if inner:
+                        s.subcycles_inner(1)
+                    else:
+                        s.subcycles(1)
                     s.exchange_pack()
                     s.exchange_unpack()
 
@@ -920,10 +929,28 @@ def run_band_timing(args, local):
                 e1.record(stream)
                 e1.synchronize()
                 out["us"].append(1000.0 * e0.elapsed_time(e1) / nsub)
+                # the step BandSolver replays: graphs of G steps whose
+                # subcycles do not end the call (no NCCL transfer here)
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.stream(stream):
+                    with torch.cuda.graph(g, stream=stream):
+                        for _ in range(G):
+                            step(inner=True)
+                g.replay()
+                s.synchronize()
+                e0, e1 = _event_pair()
+                e0.record(stream)
+                for _ in range(nsub // G):
+                    g.replay()
+                e1.record(stream)
+                e1.synchronize()
+                out["graphed_us"].append(1000.0 * e0.elapsed_time(e1) / (G * (nsub // G)))
+                del g
                 out["points"].append(b.n_own)
                 out["ring"].append(b.local.na - b.n_own)
                 out["send_bytes"].append(16 * len(b.send_idx()))
         out["max_us"] = max(out["us"])
+        out["max_graphed_us"] = max(out["graphed_us"])
         if nb == 1:
             # the same one-band step through BandSolver (graphs of 50 steps)
             # against evp1d_subcycles of the band's problem
