@@ -727,6 +727,14 @@ def ensemble_extras(local: int, steps: int, ndte: int = None) -> dict:
     - concurrent loop: every member issued at once, each on its own handle's
       stream; from an event all the streams wait on to an event that waits
       on all of them.
+    - two-kernel loop: member after member, each subcycle as the reference's
+      GPU code runs it, a stress launch then a stepu launch over the
+      member's list (evp1d_stress_only / evp1d_stepu_only, in place),
+      replayed from CUDA graphs of 50 subcycles so that no host launch
+      overhead counts; the members' device times summed.
+    - e2e: evp1d_run with page-locked host buffers (upload, subcycles,
+      download), the batched handle's one call against the members' calls
+      one after the other.
     - equal: one call of ndte from the same starting state, every output
       array of every member bit for bit between the batched handle and the
       serial loop."""
@@ -759,6 +767,19 @@ def ensemble_extras(local: int, steps: int, ndte: int = None) -> dict:
         e1.record(st_b)
         e1.synchronize()
         t_b.append(e0.elapsed_time(e1) / 1000.0)
+    # end to end from page-locked host buffers
+    fe = evp1d.FieldSet.from_problem(ens.combined, pinned=True)
+    t_be = []
+    for _ in range(steps):
+        fe.refill(ens.combined)
+        torch.cuda.synchronize()
+        e0, e1 = _event_pair()
+        e0.record(st_b)
+        s.run(ndte, fe)
+        e1.record(st_b)
+        e1.synchronize()
+        t_be.append(e0.elapsed_time(e1) / 1000.0)
+    del fe
     # equality pass, from the starting state
     fb = evp1d.FieldSet.from_problem(ens.combined)
     s.run(ndte, fb)
@@ -799,6 +820,50 @@ def ensemble_extras(local: int, steps: int, ndte: int = None) -> dict:
             h.synchronize()
             tot += e0.elapsed_time(e1) / 1000.0
         t_s.append(tot)
+    # the same serial loop end to end, from page-locked host buffers
+    fms = [evp1d.FieldSet.from_problem(m, pinned=True) for m in members]
+    t_se = []
+    for _ in range(steps):
+        tot = 0.0
+        for m, h, st, fm in zip(members, handles, streams, fms):
+            fm.refill(m)
+            e0, e1 = _event_pair()
+            e0.record(st)
+            h.run(ndte, fm)
+            e1.record(st)
+            h.synchronize()
+            tot += e0.elapsed_time(e1) / 1000.0
+        t_se.append(tot)
+    del fms
+    # the two-kernel loop: stress launch, stepu launch per subcycle
+    G = 50
+    t_2k = []
+    graphs = []
+    for h, st in zip(handles, streams):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(st):
+            with torch.cuda.graph(g, stream=st):
+                for _ in range(G):
+                    h.stress_only(1)
+                    h.stepu_only(1)
+        graphs.append(g)
+    for _ in range(steps):
+        tot = 0.0
+        for h, st, g in zip(handles, streams, graphs):
+            e0, e1 = _event_pair()
+            e0.record(st)
+            # a graph replays on torch's current stream: the member's
+            with torch.cuda.stream(st):
+                for _ in range(ndte // G):
+                    g.replay()
+                for _ in range(ndte % G):
+                    h.stress_only(1)
+                    h.stepu_only(1)
+            e1.record(st)
+            h.synchronize()
+            tot += e0.elapsed_time(e1) / 1000.0
+        t_2k.append(tot)
+    del graphs
     # concurrent loop
     side = torch.cuda.Stream(device=dev)
     t_c = []
@@ -822,12 +887,18 @@ def ensemble_extras(local: int, steps: int, ndte: int = None) -> dict:
         h.finalize()
     med = statistics.median
     b, sl_, co = units / med(t_b), units / med(t_s), units / med(t_c)
+    tk, be, se = units / med(t_2k), units / med(t_be), units / med(t_se)
     return {"config": "ens64", "members": len(members), "active_points": units // ndte,
             "ndte": ndte, "steps": steps,
-            "batched": b, "serial_loop": sl_, "concurrent_loop": co, "unit": UNIT,
+            "batched": b, "serial_loop": sl_, "concurrent_loop": co,
+            "two_kernel_loop": tk, "unit": UNIT,
             "batched_over_serial_loop": b / sl_, "batched_over_concurrent_loop": b / co,
+            "batched_over_two_kernel_loop": b / tk,
+            "e2e": {"batched": be, "serial_loop": se, "batched_over_serial_loop": be / se,
+                    "host_memory": "page-locked"},
             "ms": {"batched": 1000 * med(t_b), "serial_loop": 1000 * med(t_s),
-                   "concurrent_loop": 1000 * med(t_c)},
+                   "concurrent_loop": 1000 * med(t_c), "two_kernel_loop": 1000 * med(t_2k),
+                   "e2e_batched": 1000 * med(t_be), "e2e_serial_loop": 1000 * med(t_se)},
             "equal_bitwise_per_member": equal,
             "timing": "CUDA events on the device; serial loop = sum of the members' "
                       "device times, one member at a time"}
@@ -936,12 +1007,15 @@ def run_band_timing(args, local):
                     with torch.cuda.graph(g, stream=stream):
                         for _ in range(G):
                             step(inner=True)
-                g.replay()
+                # a graph replays on torch's current stream: the handle's
+                with torch.cuda.stream(stream):
+                    g.replay()
                 s.synchronize()
                 e0, e1 = _event_pair()
                 e0.record(stream)
-                for _ in range(nsub // G):
-                    g.replay()
+                with torch.cuda.stream(stream):
+                    for _ in range(nsub // G):
+                        g.replay()
                 e1.record(stream)
                 e1.synchronize()
                 out["graphed_us"].append(1000.0 * e0.elapsed_time(e1) / (G * (nsub // G)))

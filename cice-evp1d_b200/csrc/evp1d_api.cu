@@ -103,18 +103,21 @@ void drop_graphs(evp1d_t *h) {
   }
 }
 
-// One subcycle from buffer `from` into the other one.
-void launch_sub(evp1d_t *h, int from, bool last) {
+// One subcycle from buffer `from` into the other one.  `after_sub`: the
+// previous launch on the stream is this handle's previous subcycle (in the
+// same call or the same captured chunk).
+cudaError_t launch_sub(evp1d_t *h, int from, bool last, bool after_sub) {
   if (h->path == kPathTma) {
     evp::TmaArgs a = evp::problem_tma_args(h->d, from);
     a.prefetch = h->prefetch;
     a.trace = h->trace;
     a.nsub = 1;
     a.last = last;
-    evp::launch_tma(a, h->p, h->d.stream);
-  } else {
-    evp::launch_fused(evp::problem_fused_args(h->d, from), h->p, last, h->d.stream);
+    a.pdl = after_sub && h->pdl;
+    return evp::launch_tma(a, h->p, h->d.stream);
   }
+  evp::launch_fused(evp::problem_fused_args(h->d, from), h->p, last, h->d.stream);
+  return cudaGetLastError();
 }
 
 // A bounded device-side wait that ran out leaves a code in the error word.
@@ -134,11 +137,13 @@ int build_graph(evp1d_t *h, int from) {
   cudaGraph_t g = nullptr;
   CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   int b = from;
-  for (int k = 0; k < kGraphChunk; k++) {
-    launch_sub(h, b, false);
+  cudaError_t le = cudaSuccess;
+  for (int k = 0; k < kGraphChunk && le == cudaSuccess; k++) {
+    le = launch_sub(h, b, false, k > 0);
     b = 1 - b;
   }
   cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (e == cudaSuccess && le != cudaSuccess) e = le;
   if (e != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
     return fail(EVP1D_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
@@ -307,6 +312,7 @@ int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6]
   // subcycle before (the strip order chains the runs).
   if (const char *e = getenv("EVP1D_PERSIST"))
     h->persist = atoi(e) != 0 && evp::tma_can_persist(device, plan.nruns);
+  if (const char *e = getenv("EVP1D_PDL")) h->pdl = atoi(e) != 0;
   *handle = h;
   return EVP1D_OK;
 }
@@ -529,12 +535,15 @@ int run_subcycles(evp1d_t *h, int ndte, bool ends) {
     h->launches += kGraphChunk;
     body -= kGraphChunk;
   }
+  // a launch right after a graph launch waits for the whole graph
+  bool after_sub = false;
   for (; body > 0; body--) {
-    launch_sub(h, h->d.cur, false);
+    CUDA_TRY(launch_sub(h, h->d.cur, false, after_sub));
+    after_sub = true;
     h->d.cur = 1 - h->d.cur;
     h->launches++;
   }
-  launch_sub(h, h->d.cur, ends);
+  CUDA_TRY(launch_sub(h, h->d.cur, ends, after_sub));
   h->d.cur = 1 - h->d.cur;
   h->launches++;
   CUDA_TRY(cudaGetLastError());

@@ -135,6 +135,10 @@ template <bool kOne>
 __global__ void __launch_bounds__(kThreads, 4)  // 64 registers: 32 warps per SM
 k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__restrict__ v0,
             const double *__restrict__ u1, const double *__restrict__ v1) {
+  // launched as a programmatic dependent: the previous kernel's results
+  // (and its reads of what this one writes) are complete after the wait
+  griddep_launch_dependents();
+  griddep_wait();
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.nslots;
        x += gridDim.x * blockDim.x) {
     double lu, lv;
@@ -181,6 +185,8 @@ k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__
 template <bool kOne>
 __global__ void __launch_bounds__(kThreads, 2)
 k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__restrict__ v) {
+  griddep_launch_dependents();
+  griddep_wait();
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < a.nslots;
        w += gridDim.x * blockDim.x) {
     if (a.flags[w] & kSkipT) {  // stresses unchanged, str not written
@@ -453,10 +459,12 @@ AdjArgs adj_args(const evp1d_t *h) {
   return a;
 }
 
-// One forward subcycle between explicit state buffers.
+// One forward subcycle between explicit state buffers.  `after_sub`: the
+// previous launch on the stream is the previous subcycle's (it may then start
+// as its programmatic dependent).
 void launch_state(evp1d_t *h, double *const s_in[12], double *const s_out[12],
                   const double *u_in, const double *v_in, double *u_out, double *v_out,
-                  bool last) {
+                  bool last, bool after_sub = false) {
   DeviceProblem &d = h->d;
   if (h->path == kPathTma) {
     TmaArgs a = problem_tma_args(d, 0);
@@ -472,6 +480,7 @@ void launch_state(evp1d_t *h, double *const s_in[12], double *const s_out[12],
     a.v[1] = v_out;
     a.nsub = 1;
     a.last = last;
+    a.pdl = after_sub && h->pdl;
     launch_tma(a, h->p, d.stream);
   } else {
     FusedArgs a = problem_fused_args(d, 0);
@@ -521,7 +530,7 @@ void launch_states(evp1d_t *h, double *const s0[12], double *const s1[12], doubl
     const bool odd = i & 1;
     launch_state(h, odd ? s1 : s0, odd ? s0 : s1, tu0 + (size_t)i * entry_step,
                  tv0 + (size_t)i * entry_step, tu0 + (size_t)(i + 1) * entry_step,
-                 tv0 + (size_t)(i + 1) * entry_step, last && i == len - 1);
+                 tv0 + (size_t)(i + 1) * entry_step, last && i == len - 1, i > 0);
   }
   h->launches += len;
 }
@@ -730,14 +739,31 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
   const int grid = blocks_for(d.nslots);
   long long launches = 0;
   const bool one = A.one;
+  // Both reverse kernels start as programmatic dependents of the kernel
+  // before them (each waits for it before touching memory), so that a
+  // launch's scheduling overlaps the previous one's last blocks.
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = h->pdl ? 1 : 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = st;
+  cfg.attrs = pdl;
+  cfg.numAttrs = 1;
+  cudaError_t le = cudaSuccess;
+  auto keep = [&](cudaError_t e) {
+    if (le == cudaSuccess) le = e;
+  };
   auto reverse_step = [&](const double *u0, const double *v0, const double *u1,
                           const double *v1) {
+    const Params &p = h->p;
     if (one) {
-      k_adj_stepu<true><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0, u1, v1);
-      k_adj_stress<true><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0);
+      keep(cudaLaunchKernelEx(&cfg, k_adj_stepu<true>, a, p, u0, v0, u1, v1));
+      keep(cudaLaunchKernelEx(&cfg, k_adj_stress<true>, a, p, u0, v0));
     } else {
-      k_adj_stepu<false><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0, u1, v1);
-      k_adj_stress<false><<<grid, kThreads, 0, st>>>(a, h->p, u0, v0);
+      keep(cudaLaunchKernelEx(&cfg, k_adj_stepu<false>, a, p, u0, v0, u1, v1));
+      keep(cudaLaunchKernelEx(&cfg, k_adj_stress<false>, a, p, u0, v0));
     }
     launches += 2;
   };
@@ -772,6 +798,7 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
   else
     k_adj_final<false><<<grid, kThreads, 0, st>>>(a, A.uinit_explicit ? 0 : 1);
   launches++;
+  ADJ_TRY(le);
   ADJ_TRY(cudaGetLastError());
   A.launches = launches;
   h->launches += launches;

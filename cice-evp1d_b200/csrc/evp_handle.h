@@ -29,6 +29,11 @@ struct evp1d_handle {
   // TMA path: a call's subcycles in one launch whose CTAs stay resident
   // (cooperative), instead of one launch per subcycle in CUDA graphs
   bool persist = false;
+  // TMA path: each subcycle's launch after the first of a call (and of a
+  // captured chunk) is a programmatic dependent of the one before, so that
+  // its prologue overlaps the previous launch's last tiles (EVP1D_PDL=0
+  // turns it off)
+  bool pdl = true;
   long long *trace = nullptr;  // device timing trace (EVP1D_TRACE, debug)
   bool uploaded = false;
   bool uinit_explicit = false;  // the last upload gave uvel_init/vvel_init

@@ -10,6 +10,20 @@
 
 namespace evp {
 
+// Programmatic dependent launch.  launch_dependents lets the next launch on
+// the stream (when it was launched as a programmatic dependent) be scheduled
+// once every CTA of this one has executed it or exited; its CTAs then take
+// the room this launch's CTAs leave.  wait blocks until the previous launch
+// has completed and its memory is visible (it returns at once in a launch
+// that is not a programmatic dependent).
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+__device__ __forceinline__ void griddep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Skip flags packed per slot: bit 0 = skipT, bit 1 = skipU.  Alignment
 // padding slots carry both bits.
 constexpr uint8_t kSkipT = 1;
@@ -125,6 +139,11 @@ struct TmaArgs {
   const int32_t *dep_off = nullptr, *dep_idx = nullptr;
   int *err = nullptr;  // nonzero after a bounded wait ran out
   int prefetch = 0;    // tiles prefetched into L2 ahead of the shared ring
+  // Launch as a programmatic dependent of the previous launch on the stream
+  // (one-subcycle launches only).  The previous launch must be the preceding
+  // subcycle's k_tma over the same plan: the dependent reads the records and
+  // constant blocks before that launch has completed, the state after.
+  bool pdl = false;
   // optional timing trace of block 0 (debug): per tile 8 %globaltimer stamps
   // [0] producers issued all copies, [1] consumer 0 has the stress part,
   // [2] stress done (consumer barrier), [3] bulk warp has the tile record,

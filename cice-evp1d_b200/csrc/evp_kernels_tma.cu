@@ -290,6 +290,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   }
   if (tid < 24) S.str[tid >> 3][tid & 7][kZeroSlot] = 0.0;
   __syncthreads();
+  // A launch of one subcycle may be followed by the next subcycle's, launched
+  // as a programmatic dependent (a.pdl there): it can start as soon as every
+  // CTA here has started.  Its CTAs cannot share an SM with these (shared
+  // memory), so they take the SMs these CTAs leave, and before their
+  // griddep_wait they read only what no subcycle writes (tile records,
+  // constant blocks).
+  if (!kMulti) griddep_launch_dependents();
 
   const int T0 = a.run_off[blockIdx.x], T1 = a.run_off[blockIdx.x + 1];
   const int n = T1 - T0;             // tiles of the run
@@ -446,22 +453,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       const int off = rec[0], cnt = rec[1], nx = rec[2], nh = rec[3];
       if (pw == 0) {
         const uint32_t b8 = (uint32_t)((cnt + 3) & ~3) * 8u;
-        if (lane == 0)
+        if (lane == 0) {
           bulk_g2s(st.cs, a.cblk + (size_t)t * kBlk, kCsBytes, &S.sfull[s]);
-        else if (lane <= 12)
+          // a programmatic dependent has the time: the first stepu part
+          // goes out before the state, while the previous launch drains
+          if (issued == 0 && a.pdl) issue_stepu(nu++);
+        }
+        // the state the previous subcycle wrote
+        if (issued == 0) griddep_wait();
+        if (lane >= 1 && lane <= 12)
           bulk_g2s(st.s12[lane - 1], a.s[from][lane - 1] + off, b8, &S.sfull[s]);
         else if (lane == 13)
           bulk_g2s(st.u, u_in + off, b8, &S.sfull[s]);
         else if (lane == 14)
           bulk_g2s(st.v, v_in + off, b8, &S.sfull[s]);
         if (lane == 0) {
-          if (issued == 0) issue_stepu(nu++);
+          if (issued == 0 && nu == 0) issue_stepu(nu++);
           trace_stamp(a, issued, 6);
         }
       } else {
         // gather warp gw takes the velocity extras u (first) / v (last) and
         // every kGatherWarps-th halo field; the last one also the halo meta
         const int gw = pw - 1;
+        if (issued == 0) griddep_wait();
         if (!multi) {
           if (gw == 0)
             for (int x = lane; x < nx; x += 32)
@@ -578,6 +592,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   const int c = tid;  // compute-set index: owned c < cnt, halo cnt + h
   const int lane = tid & 31;
   bool fail = false;
+  // Consumers write the ping-pong set the previous subcycle read: only after
+  // it has completed (their first tile cannot land before that anyway).
+  griddep_wait();
 
 
   // What stepu of a tile needs from its stress part, kept by the owned
@@ -675,21 +692,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     const bool wlast = kMulti ? (a.last && sub == a.nsub - 1) : kLast;
     const bool hu = mbar_wait(&S.ufull, (uint32_t)q & 1, a.err, 11);
     fail |= !hu;
-    if (hu && c < cy.cnt && !((cy.m >> 30) & kSkipU)) {
-      const uint32_t m = cy.m;
+    const bool act = hu && c < cy.cnt && !((cy.m >> 30) & kSkipU);
+    // the 13 stepu inputs into registers first, so that the stepu slot is
+    // released before the arithmetic: the bulk warp then issues the next
+    // tile's stepu part and, behind it, the stress part after next a whole
+    // stepu earlier.  (In a launch of several subcycles the release also
+    // tells the bulk warp that the tile's velocities are stored, which it
+    // publishes to other CTAs: there it stays after the stores.)
+    StepuIn in;
+    if (act) {
       const USlot &us = S.us;
-      const double(&str)[8][kStrRow] = S.str[b];
-      // a neighbour's str: own table, or the previous tile's (kStrPrev)
-      const uint32_t vnw = m & kLnbMask, vsw = (m >> kLnbBits) & kLnbMask;
-      const uint32_t vsse = (m >> (2 * kLnbBits)) & kLnbMask;
-      const double(&tnw)[8][kStrRow] = (vnw & kStrPrev) ? S.str[bp] : S.str[b];
-      const double(&tsw)[8][kStrRow] = (vsw & kStrPrev) ? S.str[bp] : S.str[b];
-      const double(&tsse)[8][kStrRow] = (vsse & kStrPrev) ? S.str[bp] : S.str[b];
-      const int lnw = vnw & (kStrPrev - 1), lsw = vsw & (kStrPrev - 1);
-      const int lsse = vsse & (kStrPrev - 1);
-      StepuIn in;
-      in.uold = cy.uold;
-      in.vold = cy.vold;
       in.kvrel = us.cu[0][c];
       in.uocn = us.cu[1][c];
       in.vocn = us.cu[2][c];
@@ -703,6 +715,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       in.Tbu = us.cu[10][c];
       in.uinit = us.cu[11][c];
       in.vinit = us.cu[12][c];
+    }
+    if (!kMulti) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&S.uempty);  // this warp is done with the stepu slot
+    }
+    if (act) {
+      const uint32_t m = cy.m;
+      const double(&str)[8][kStrRow] = S.str[b];
+      // a neighbour's str: own table, or the previous tile's (kStrPrev)
+      const uint32_t vnw = m & kLnbMask, vsw = (m >> kLnbBits) & kLnbMask;
+      const uint32_t vsse = (m >> (2 * kLnbBits)) & kLnbMask;
+      const double(&tnw)[8][kStrRow] = (vnw & kStrPrev) ? S.str[bp] : S.str[b];
+      const double(&tsw)[8][kStrRow] = (vsw & kStrPrev) ? S.str[bp] : S.str[b];
+      const double(&tsse)[8][kStrRow] = (vsse & kStrPrev) ? S.str[bp] : S.str[b];
+      const int lnw = vnw & (kStrPrev - 1), lsw = vsw & (kStrPrev - 1);
+      const int lsse = vsse & (kStrPrev - 1);
+      in.uold = cy.uold;
+      in.vold = cy.vold;
       in.s1 = str[0][c];
       in.s2nw = tnw[1][lnw];
       in.s3sse = tsse[2][lsse];
@@ -722,8 +752,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
         a.Cb[cy.off + c] = o.Cb;
       }
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&S.uempty);  // this warp is done with the stepu slot
+    if (kMulti) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&S.uempty);
+    }
     if (tid == 0) trace_stamp(a, q, 5);
   };
 
@@ -851,6 +883,21 @@ cudaError_t launch_tma(const TmaArgs &a, const Params &p, cudaStream_t st) {
   if (a.nsub != 1) return cudaErrorInvalidValue;  // several subcycles need the counters
   TmaKernel k = a.last ? (std ? k_tma<true, true, false> : k_tma<true, false, false>)
                        : (std ? k_tma<false, true, false> : k_tma<false, false, false>);
+  if (a.pdl) {
+    // a programmatic dependent of the previous launch on the stream, which
+    // must be the previous subcycle's k_tma (the caller's guarantee)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(a.nruns);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem_bytes();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, a, p);
+  }
   k<<<a.nruns, kThreads, smem_bytes(), st>>>(a, p);
   return cudaGetLastError();
 }

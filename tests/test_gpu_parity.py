@@ -328,13 +328,16 @@ def test_plan_shapes_bitwise(oracle_mod, monkeypatch, strip_w, runs):
     assert_same(gpu_run(pr, 7), oracle_run(oracle_mod, pr, 7), pr)
 
 
-@pytest.mark.parametrize("persist", ["0", "1"])
+@pytest.mark.parametrize("persist,pdl", [("0", "1"), ("0", "0"), ("1", "1")])
 @pytest.mark.parametrize("ndte", [1, 2, 3, 49, 50, 51, 101])
-def test_launch_modes_bitwise(oracle_mod, monkeypatch, persist, ndte):
+def test_launch_modes_bitwise(oracle_mod, monkeypatch, persist, pdl, ndte):
     """A call's subcycles in one multi-subcycle launch (CTAs resident, per-tile
-    counters between subcycles) or one launch per subcycle in graphs of 50:
-    the same bits, for odd and even counts and around the graph chunk."""
+    counters between subcycles) or one launch per subcycle in graphs of 50,
+    each launch after the first of a call or chunk a programmatic dependent
+    of the one before (pdl) or not: the same bits, for odd and even counts
+    and around the graph chunk."""
     monkeypatch.setenv("EVP1D_PERSIST", persist)
+    monkeypatch.setenv("EVP1D_PDL", pdl)
     pr = synth.to_1d(synth.make_grid(97, 61, seed=31, ndte=ndte, curvilinear=True))
     assert_same(gpu_run(pr, ndte, calls=1), oracle_run(oracle_mod, pr, ndte), pr)
 
