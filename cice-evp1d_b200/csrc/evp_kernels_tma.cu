@@ -22,8 +22,14 @@
 // the new stresses and velocities to the other ping-pong buffer.  Stepu reads
 // str from the tile's own table and from the previous tile's, which stays
 // alive: three str tables rotate, so that one tile's stress can start while
-// stepu still reads the two before it.  The 13 stepu inputs of a point come
-// straight from its constant block into the thread's registers, a tile ahead.
+// stepu still reads the two before it.  The 13 stepu inputs of a tile (the
+// second part of its constant block) arrive by one more bulk copy into a
+// stepu slot, which the consumers release as soon as each has its point's
+// inputs in registers.
+// Consecutive one-subcycle launches overlap: each CTA lets the next launch
+// start at once (griddepcontrol.launch_dependents), and a launch started that
+// way loads its first tile's records, constants and stepu part while the
+// previous one finishes, reading the state only after griddepcontrol.wait.
 //
 // Every mbarrier wait is bounded by %globaltimer (kWaitNs): on expiry the
 // kernel records an error code, every thread of the consumer group leaves the
