@@ -438,6 +438,9 @@ def run_adjoint(args, rank, world, local):
         return f.uvel[:na].copy(), f.vvel[:na].copy()
 
     def central(k, d, step):
+        """Central difference of J along d, and the adjoint's derivative
+        along the perturbation the two runs actually received (the rounded
+        x +- step*d), both divided by 2 step."""
         prp, prm = pr.copy(), pr.copy()
         prp.f[k] = pr.f[k] + step * d
         prm.f[k] = pr.f[k] - step * d
@@ -445,23 +448,32 @@ def run_adjoint(args, rank, world, local):
         um, vm = run(prm)
         # summed point by point so that the difference does not cancel
         # against the size of J
-        return float(np.sum((up - um) * (up + um - 2 * uobs) +
-                            (vp - vm) * (vp + vm - 2 * vobs))) / (2 * step)
+        fd_ = float(np.sum((up - um) * (up + um - 2 * uobs) +
+                           (vp - vm) * (vp + vm - 2 * vobs))) / (2 * step)
+        ad_ = float(np.dot(g[k], prp.f[k] - prm.f[k])) / (2 * step)
+        return fd_, ad_
 
     # central differences at relative steps 1e-4 .. 1e-7, 8 directions per
     # field: truncation error falls with the step, rounding error grows, and
     # the best step shows how close the adjoint is
     steps = (1e-4, 1e-5, 1e-6, 1e-7)
     fd = {k: {str(st_): 0.0 for st_ in steps} for k in ("strength", "Cw", "forcex", "forcey")}
+    errs_h = {k: [] for k in fd}  # every direction's error at the step h
     for k in fd:
         for _ in range(8):
             d = pr.f[k] * rng.standard_normal(na)
-            ad = float(np.dot(g[k], d))
             for st_ in steps:
-                e = abs(central(k, d, st_) - ad) / abs(ad)
+                fd_, ad_ = central(k, d, st_)
+                e = abs(fd_ - ad_) / abs(ad_)
                 fd[k][str(st_)] = max(fd[k][str(st_)], e)
+                if st_ == h:
+                    errs_h[k].append(e)
     fd_err = {k: v[str(h)] for k, v in fd.items()}
     fd_best = {k: min(v.values()) for k, v in fd.items()}
+    all_h = [e for v in errs_h.values() for e in v]
+    fd_dirs = {"median_rel_err": float(np.median(all_h)),
+               "within_1e-6": int(sum(e <= 1e-6 for e in all_h)), "of": len(all_h),
+               "by_field": {k: sorted(v) for k, v in errs_h.items()}}
     s.finalize()
 
     med = statistics.median
@@ -492,6 +504,7 @@ def run_adjoint(args, rank, world, local):
                              "adjoint_work": info["work_bytes"],
                              "forward_solver": info["solver_bytes"]},
             "fd_check": {"directions": 32, "step": h, "max_rel_err": fd_err,
+                         "directions_at_step": fd_dirs,
                          "max_rel_err_by_step": fd, "best_step_max_rel_err": fd_best},
             "gpu_launches": launches,
             "clocks": sampler.summary() if sampler else None,

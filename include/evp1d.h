@@ -176,8 +176,9 @@ int evp1d_synchronize(evp1d_t *handle);
  * and clears it; the handle stays usable. */
 int evp1d_debug_wait_timeout(evp1d_t *handle, long long ns);
 
-/* Debug: the same for the other bounded wait of the solver.  A call's
- * subcycles run in one launch whose CTAs stay resident; before a tile loads
+/* Debug: the same for the other bounded wait of the solver.  With
+ * EVP1D_PERSIST=1 a call's subcycles run in one launch whose CTAs stay
+ * resident (by default each subcycle is a launch of its own); before a tile loads
  * the next subcycle's state, its CTA waits on per-tile counters until the
  * tiles it depends on have finished the subcycle before.  This queues one
  * such wait on a counter that nothing raises, limited to `ns` nanoseconds
