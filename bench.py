@@ -303,7 +303,8 @@ def run_ensemble(args, rank, world, local):
         h.finalize()
     value = units_all * args.steps / t_b
     loop_value = units_all * args.steps / t_l
-    ab = alg_bytes.per_point_subcycle(path)
+    short = all(alg_bytes.short_stepu(m, _params_revp(ndte)) for m in members)
+    ab = alg_bytes.per_point_subcycle(path, short)
     units_rank = sum(m.n_active for m in members) * ndte
     achieved = ab * (units_rank / ndte) / (t_b / (args.steps * ndte)) / 1e9
     peak, peak_src = alg_bytes.hbm_peak(ROOT)
@@ -691,7 +692,7 @@ def run_split(args, rank, world, local):
     h2d, d2h = reduce(h2d, SUM), reduce(d2h, SUM)
     sent = reduce(16 * len(band.send_idx()), SUM)
     ring = reduce(band.local.na - band.n_own, SUM)
-    ab = alg_bytes.per_point_subcycle(s.path)
+    ab = alg_bytes.per_point_subcycle(s.path, alg_bytes.short_stepu(band.local, _params_revp(ndte)))
     sub_s = t_dev / (args.steps * ndte)
     achieved = ab * band.local.na / sub_s / 1e9
     peak, peak_src = alg_bytes.hbm_peak(ROOT)
@@ -727,6 +728,13 @@ def run_split(args, rank, world, local):
 def _event_pair():
     import torch
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _params_revp(ndte: int) -> float:
+    """revp of the parameters the bench's handles run with (the defaults of
+    evp1d_set_evp_parameters)."""
+    import evp1d
+    return float(evp1d.set_evp_parameters(ndte).revp)
 
 
 def ensemble_extras(local: int, steps: int, ndte: int = None) -> dict:
@@ -1156,7 +1164,8 @@ def main():
     value = n_active_all * ndte * args.steps / t_max
 
     # ---------------- roofline of the subcycle ----------------
-    ab = alg_bytes.per_point_subcycle(solver.path)
+    short = alg_bytes.short_stepu(pr, _params_revp(ndte))
+    ab = alg_bytes.per_point_subcycle(solver.path, short)
     sub_s = t_dev / (args.steps * ndte)
     achieved = ab * pr.n_active / sub_s / 1e9
     peak, peak_src = alg_bytes.hbm_peak(ROOT)
@@ -1251,6 +1260,8 @@ def main():
                          "peak_source": peak_src,
                          "algorithmic_bytes_per_point_subcycle": ab,
                          "kernel": path,
+                         "stepu_part": ("short: Tbu +0, uvel_init/vvel_init finite, revp 0"
+                                        if short else "full"),
                          # the same rate over the reference's unfused data
                          # contract (str1..8 through HBM, 576 B): what the
                          # reference's two kernels would have to move

@@ -479,8 +479,7 @@ int evp1d_set_params(evp1d_t *h, const evp1d_params *params) {
   if (h->uploaded && h->p.rhow != old_rhow && h->d.nslots > 0) {
     evp::launch_drag_factor(h->d.nslots, h->d.dyn[evp::kAiu], h->d.dyn[evp::kCw],
                             h->p.rhow, h->d.dyn[evp::kKvrel], h->d.stream);
-    evp::problem_fill_const(&h->d);
-    CUDA_TRY(cudaGetLastError());
+    CHECK(evp::problem_fill_const(&h->d));
   }
   return EVP1D_OK;
 }

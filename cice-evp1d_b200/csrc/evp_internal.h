@@ -69,6 +69,9 @@ struct DeviceProblem {
   int32_t *tile_rec = nullptr;   // kRecInts int32 per tile (producer records)
   double *cblk = nullptr;        // per-call constants, kConstFields x 256 per tile
   int *err = nullptr;        // device error word of the bounded waits
+  // device word of launch_const_blocks' field checks: 0 when every Tbu of the
+  // call is +0 and every uinit, vinit finite (TmaArgs::compact)
+  int *cflags = nullptr;
   int nctas = 0;             // SM count of the device
   uint8_t *flags = nullptr;
   double *geo[kNumGeo] = {};
@@ -101,8 +104,9 @@ int problem_upload_staged(DeviceProblem *d, bool uinit_given, bool vinit_given, 
 // 15 strinty, 16 Cb, 17 + k str_k when want_str[k]).
 int problem_download_staged(DeviceProblem *d, const bool want_str[8]);
 // Rebuild the per-tile constant blocks from the slot arrays (after the
-// per-call fields or the drag factor changed).
-void problem_fill_const(DeviceProblem *d);
+// per-call fields or the drag factor changed), with the field checks in
+// cflags.
+int problem_fill_const(DeviceProblem *d);
 // Results device -> host; waits for the stream.
 int problem_download(DeviceProblem *d, const evp1d_fields *io);
 

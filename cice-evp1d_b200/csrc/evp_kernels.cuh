@@ -94,6 +94,12 @@ void launch_fused(const FusedArgs &a, const Params &p, bool last,
 // come from the constant blocks.
 constexpr int kTmaStressFields = 19;
 constexpr int kTmaStepuFields = 13;
+// The stepu part without its last three fields (Tbu, uinit, vinit): enough
+// when every Tbu of the call is +0 and every uinit, vinit is finite, and
+// revp == 0 (TmaArgs::compact).  stepu then takes Tbu = +0, which is the
+// value, and uinit = +-1 with uinit's sign (bits 62 and 63 of the packed
+// word): revp*uinit is the same signed zero either way.
+constexpr int kTmaStepuCompact = 10;
 // Per-call constants of a tile in one contiguous block: kConstFields x
 // kTileOwned doubles per tile, fields [0..5] dxT dyT HTE HTN HTEm1 HTNm1,
 // [6] strength, [7] meta | lcor << 32 (the kConstStressFields that stress
@@ -144,6 +150,12 @@ struct TmaArgs {
   // subcycle's k_tma over the same plan: the dependent reads the records and
   // constant blocks before that launch has completed, the state after.
   bool pdl = false;
+  // The stepu part may be the first kTmaStepuCompact fields (see there):
+  // where `compact` is set, *cflags is 0 (the call's fields allow it; read
+  // by the kernel, so captured launches stay valid across uploads) and
+  // revp == 0 (checked at launch).
+  bool compact = false;
+  const int *cflags = nullptr;
   // optional timing trace of block 0 (debug): per tile 8 %globaltimer stamps
   // [0] producers issued all copies, [1] consumer 0 has the stress part,
   // [2] stress done (consumer barrier), [3] bulk warp has the tile record,
@@ -195,11 +207,13 @@ void launch_flags(int nslots, const int32_t *point_of_slot,
                   const int32_t *skipT, const int32_t *skipU, uint8_t *flags,
                   const uint32_t *lnb, uint32_t *meta, cudaStream_t st);
 // cblk[(t*kConstFields + f)*256 + l] for l < tile_cnt[t] and slot
-// s = tile_off[t] + l: src[f][s] for f < 7, meta[s] | lcor[s] << 32 for f = 7,
-// src[f-1][s] for f >= 8; 0 for l >= tile_cnt[t].
+// s = tile_off[t] + l: src[f][s] for f < 7, meta[s] | lcor[s] << 32 with the
+// sign bits of uinit (src[18]) and vinit (src[19]) in bits 62 and 63 for
+// f = 7, src[f-1][s] for f >= 8; 0 for l >= tile_cnt[t].  *cflags gets bit 0
+// if a Tbu (src[17]) is not +0 and bit 1 if a uinit or vinit is not finite.
 void launch_const_blocks(int ntiles, const int32_t *tile_off, const int32_t *tile_cnt,
                          const double *const src[kConstFields - 1], const uint32_t *meta,
-                         const uint32_t *lcor, double *cblk, cudaStream_t st);
+                         const uint32_t *lcor, double *cblk, int *cflags, cudaStream_t st);
 // kvrel[s] = (aiu[s]*rhow)*Cw[s].
 void launch_drag_factor(int nslots, const double *aiu, const double *Cw,
                         double rhow, double *kvrel, cudaStream_t st);

@@ -216,8 +216,11 @@ struct ConstSrc {
 
 __global__ void k_const_blocks(int ntiles, const int32_t *tile_off, const int32_t *tile_cnt,
                                ConstSrc src, const uint32_t *meta, const uint32_t *lcor,
-                               double *cblk) {
+                               double *cblk, int *cflags) {
+  constexpr int kTbuSrc = kConstFields - 4, kUinitSrc = kConstFields - 3;
+  constexpr int kVinitSrc = kConstFields - 2;
   const long long total = (long long)ntiles * kConstFields * kConstTileSlots;
+  int flags = 0;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const int l = (int)(e % kConstTileSlots);
@@ -227,27 +230,37 @@ __global__ void k_const_blocks(int ntiles, const int32_t *tile_off, const int32_
     double v = 0.0;
     if (l < tile_cnt[t]) {
       const int s = tile_off[t] + l;
-      if (f == kConstStressFields - 1)
+      if (f == kConstStressFields - 1) {
+        const unsigned long long su =
+            (unsigned long long)__double_as_longlong(src.f[kUinitSrc][s]) >> 63;
+        const unsigned long long sv =
+            (unsigned long long)__double_as_longlong(src.f[kVinitSrc][s]) >> 63;
         v = __longlong_as_double((long long)((unsigned long long)meta[s] |
-                                             ((unsigned long long)lcor[s] << 32)));
-      else
-        v = src.f[f < kConstStressFields ? f : f - 1][s];
+                                             ((unsigned long long)lcor[s] << 32) | su << 62 |
+                                             sv << 63));
+      } else {
+        const int k = f < kConstStressFields ? f : f - 1;
+        v = src.f[k][s];
+        if (k == kTbuSrc && __double_as_longlong(v) != 0) flags |= 1;
+        if ((k == kUinitSrc || k == kVinitSrc) && !isfinite(v)) flags |= 2;
+      }
     }
     cblk[e] = v;
   }
+  if (flags) atomicOr(cflags, flags);
 }
 }  // namespace
 
 void launch_const_blocks(int ntiles, const int32_t *tile_off, const int32_t *tile_cnt,
                          const double *const src[kConstFields - 1], const uint32_t *meta,
-                         const uint32_t *lcor, double *cblk, cudaStream_t st) {
+                         const uint32_t *lcor, double *cblk, int *cflags, cudaStream_t st) {
   if (ntiles <= 0) return;
   ConstSrc cs;
   for (int f = 0; f < kConstFields - 1; f++) cs.f[f] = src[f];
   const long long total = (long long)ntiles * kConstFields * kConstTileSlots;
   const long long b = (total + 255) / 256;
-  k_const_blocks<<<(int)(b < 148 * 32 ? b : 148 * 32), 256, 0, st>>>(ntiles, tile_off, tile_cnt,
-                                                                      cs, meta, lcor, cblk);
+  k_const_blocks<<<(int)(b < 148 * 32 ? b : 148 * 32), 256, 0, st>>>(
+      ntiles, tile_off, tile_cnt, cs, meta, lcor, cblk, cflags);
 }
 
 }  // namespace evp

@@ -303,6 +303,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   // griddep_wait they read only what no subcycle writes (tile records,
   // constant blocks).
   if (!kMulti) griddep_launch_dependents();
+  // the short stepu part (kTmaStepuCompact fields) where the call allows it
+  const bool cpt = a.compact && __ldg(a.cflags) == 0;
 
   const int T0 = a.run_off[blockIdx.x], T1 = a.run_off[blockIdx.x + 1];
   const int n = T1 - T0;             // tiles of the run
@@ -343,13 +345,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
     const int pw = (tid - kConsumers) >> 5;
     const int lane = tid & 31;
     constexpr uint32_t kRecBytes = kRecInts * 4u;
-    constexpr uint32_t kUBytes = kTmaStepuFields * kTileOwned * 8u;
+    const uint32_t ubytes = (cpt ? kTmaStepuCompact : kTmaStepuFields) * kTileOwned * 8u;
     auto issue_stepu = [&](int q) {  // lane 0 of the bulk warp
-      mbar_arrive_expect_tx(&S.ufull, kUBytes);
+      mbar_arrive_expect_tx(&S.ufull, ubytes);
       bulk_g2s(S.us.cu,
                a.cblk + ((size_t)(T0 + (kMulti ? q % n : q)) * kConstFields + kConstStressFields) *
                             kTileOwned,
-               kUBytes, &S.ufull);
+               ubytes, &S.ufull);
     };
     int pub = 0;  // steps whose counters are raised (multi-subcycle launches)
     int nu = 0;   // stepu parts issued (the bulk warp's lane 0 counts)
@@ -607,6 +609,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
   // thread so that the slot can be released after stress.
   struct Carry {
     uint32_t m = 0;
+    uint32_t sg = 0;  // sign bits of uinit (bit 0) and vinit (bit 1)
     double uold = 0.0, vold = 0.0;
     int off = 0, cnt = 0;
   };
@@ -636,6 +639,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
           m = (uint32_t)ml;
           lc = (uint32_t)(ml >> 32);
           cy.m = m;
+          cy.sg = lc >> 30;
           cy.uold = st.u[c];
           cy.vold = st.v[c];
         } else {
@@ -718,9 +722,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
       in.umassdti = us.cu[7][c];
       in.fm = us.cu[8][c];
       in.uarear = us.cu[9][c];
-      in.Tbu = us.cu[10][c];
-      in.uinit = us.cu[11][c];
-      in.vinit = us.cu[12][c];
+      if (cpt) {
+        // Tbu is +0; revp == 0, so revp*uinit is a zero with uinit's sign
+        in.Tbu = 0.0;
+        in.uinit = (cy.sg & 1u) ? -1.0 : 1.0;
+        in.vinit = (cy.sg & 2u) ? -1.0 : 1.0;
+      } else {
+        in.Tbu = us.cu[10][c];
+        in.uinit = us.cu[11][c];
+        in.vinit = us.cu[12][c];
+      }
     }
     if (!kMulti) {
       __syncwarp();
@@ -874,8 +885,11 @@ bool tma_can_persist(int device, int nruns) {
   return coop != 0 && nruns <= sms * per_sm;
 }
 
-cudaError_t launch_tma(const TmaArgs &a, const Params &p, cudaStream_t st) {
-  if (a.ntiles <= 0 || a.nruns <= 0 || a.nsub <= 0) return cudaSuccess;
+cudaError_t launch_tma(const TmaArgs &given, const Params &p, cudaStream_t st) {
+  if (given.ntiles <= 0 || given.nruns <= 0 || given.nsub <= 0) return cudaSuccess;
+  TmaArgs a = given;
+  // the short stepu part replaces revp*uinit by a signed zero: revp == 0 only
+  a.compact = given.compact && given.cflags && p.revp == 0.0;
   const bool std = std_params(p);
   if (a.nsub > 1 && a.epoch) {
     // CTAs wait on one another: all of them resident at once

@@ -1,5 +1,6 @@
 // evp_problem.cu -- device arena of one 1D problem and its movement between
 // the caller's reference-order host arrays and the slot-ordered device state.
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -54,6 +55,7 @@ void layout(DeviceProblem *d, Carve &c, size_t nhalo_total, size_t nuvx_total,
             size_t ndep_total) {
   const size_t S = (size_t)d->nslots, U = (size_t)d->nuv, T = (size_t)d->ntiles;
   c.take(&d->err, 1);
+  c.take(&d->cflags, 1);
   c.take(&d->meta, S);
   c.take(&d->lcor, S);
   c.take(&d->halo_lcc, nhalo_total);
@@ -289,7 +291,7 @@ int problem_upload_staged(DeviceProblem *d, bool uinit_given, bool vinit_given, 
     }
   }
   launch_drag_factor(d->nslots, d->dyn[kAiu], d->dyn[kCw], rhow, d->dyn[kKvrel], st);
-  problem_fill_const(d);
+  TRY(problem_fill_const(d));
   for (int k = 0; k < 8; k++)
     CUDA_TRY(cudaMemsetAsync(d->str[k], 0, (size_t)d->nuv * sizeof(double), st));
   CUDA_TRY(cudaGetLastError());
@@ -298,15 +300,18 @@ int problem_upload_staged(DeviceProblem *d, bool uinit_given, bool vinit_given, 
   return EVP1D_OK;
 }
 
-void problem_fill_const(DeviceProblem *d) {
-  if (d->ntiles == 0) return;
+int problem_fill_const(DeviceProblem *d) {
+  if (d->ntiles == 0) return EVP1D_OK;
   const double *src[kConstFields - 1] = {
       d->geo[kDxT],  d->geo[kDyT],    d->geo[kHTE],    d->geo[kHTN],    d->geo[kHTEm1],
       d->geo[kHTNm1], d->dyn[kStrength], d->dyn[kKvrel], d->dyn[kUocn], d->dyn[kVocn],
       d->dyn[kWaterx], d->dyn[kWatery], d->dyn[kForcex], d->dyn[kForcey], d->dyn[kUmassdti],
       d->dyn[kFm],   d->geo[kUarear], d->dyn[kTbu],    d->dyn[kUinit],  d->dyn[kVinit]};
+  CUDA_TRY(cudaMemsetAsync(d->cflags, 0, sizeof(int), d->stream));
   launch_const_blocks(d->ntiles, d->tile_off, d->tile_cnt, src, d->meta, d->lcor, d->cblk,
-                      d->stream);
+                      d->cflags, d->stream);
+  CUDA_TRY(cudaGetLastError());
+  return EVP1D_OK;
 }
 
 int problem_download(DeviceProblem *d, const evp1d_fields *io) {
@@ -485,6 +490,15 @@ TmaArgs problem_tma_args(const DeviceProblem &d, int from) {
   for (int k = 0; k < 6; k++) a.sg[k] = d.geo[geo_order[k]];
   a.sg[6] = d.dyn[kStrength];
   a.cblk = d.cblk;
+  a.cflags = d.cflags;
+  // the short stepu part where the call's fields allow it (EVP1D_COMPACT=0: never)
+  {
+    static const bool allowed = [] {
+      const char *e = getenv("EVP1D_COMPACT");
+      return !(e && atoi(e) == 0);
+    }();
+    a.compact = allowed;
+  }
   a.u[0] = d.u[from];
   a.v[0] = d.v[from];
   a.u[1] = d.u[to];

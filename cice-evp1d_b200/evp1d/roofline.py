@@ -21,7 +21,11 @@ once and neighbour gathers served from cache:
   neighbours: 48 * 8 + 1 + 12 + 4 = 401 B.  The recomputed forward halo is
   not algorithmic and shows up only in the measured traffic.
 * ``fused-tile-tma`` -- the same data flow with the tile's fields staged into
-  shared memory by TMA bulk copies: 401 B.
+  shared memory by TMA bulk copies: 401 B.  When every Tbu of the call is +0,
+  every uvel_init and vvel_init finite and revp == 0, stepu needs neither Tbu
+  nor uvel_init, vvel_init (Tbu is +0, and revp*uvel_init a signed zero whose
+  sign the kernel takes from a bit of the packed index word), and the kernel
+  copies a stepu part without them: 401 - 3 * 8 = 377 B (``short_stepu``).
 """
 from __future__ import annotations
 
@@ -37,8 +41,31 @@ BYTES_PER_POINT_SUBCYCLE = {
 FALLBACK_HBM_GBS = 6650.0
 
 
-def per_point_subcycle(path: str) -> int:
-    return BYTES_PER_POINT_SUBCYCLE[path]
+SHORT_STEPU_SAVING = 3 * 8  # Tbu, uvel_init, vvel_init
+
+
+def per_point_subcycle(path: str, short: bool = False) -> int:
+    """Algorithmic bytes per point-subcycle of a kernel path; `short`: the
+    call lets the TMA path copy the short stepu part (short_stepu)."""
+    b = BYTES_PER_POINT_SUBCYCLE[path]
+    return b - SHORT_STEPU_SAVING if short and path == "fused-tile-tma" else b
+
+
+def short_stepu(pr, revp: float, explicit_init: bool = False) -> bool:
+    """Whether a call of problem `pr` lets the TMA path copy the short stepu
+    part: every Tbu +0 (bit pattern 0), every uvel_init and vvel_init finite
+    (the call-start velocities unless given), revp == 0, and the part not
+    turned off with EVP1D_COMPACT=0."""
+    import numpy as np
+    if os.environ.get("EVP1D_COMPACT", "1").strip() == "0" or revp != 0.0:
+        return False
+    na = pr.na
+    tbu = np.ascontiguousarray(pr.f["Tbu"][:na], dtype=np.float64)
+    if np.any(tbu.view(np.int64) != 0):
+        return False
+    ui = pr.f["uvel_init"][:na] if explicit_init else pr.uvel[:na]
+    vi = pr.f["vvel_init"][:na] if explicit_init else pr.vvel[:na]
+    return bool(np.all(np.isfinite(ui)) and np.all(np.isfinite(vi)))
 
 
 def hbm_peak(root: str):

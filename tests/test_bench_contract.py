@@ -41,3 +41,28 @@ def test_reference_arm_other_ranks_exit_quietly():
     r = _run({"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [l for l in r.stdout.splitlines() if l.strip().startswith("{")]
+
+
+def test_short_stepu_condition(monkeypatch):
+    """The roofline's byte count follows the kernel's choice of stepu part:
+    377 B when every Tbu is +0, every uvel_init/vvel_init finite and
+    revp == 0, else 401 B."""
+    import numpy as np
+    from evp1d import synth, roofline
+    pr = synth.make_problem("grid400x300", nx=40, ny=30, ndte=3)
+    assert roofline.short_stepu(pr, 0.0)
+    assert roofline.per_point_subcycle("fused-tile-tma", True) == 377
+    assert roofline.per_point_subcycle("fused-tile-tma", False) == 401
+    assert roofline.per_point_subcycle("fused-tile", True) == 401
+    assert not roofline.short_stepu(pr, 1.0)
+    q = pr.copy()
+    q.f["Tbu"] = q.f["Tbu"].copy()
+    q.f["Tbu"][3] = -0.0
+    assert not roofline.short_stepu(q, 0.0)
+    q = pr.copy()
+    q.f["uvel_init"] = q.f["uvel_init"].copy()
+    q.f["uvel_init"][5] = np.inf
+    assert roofline.short_stepu(q, 0.0)  # defaulted: the call-start velocities
+    assert not roofline.short_stepu(q, 0.0, explicit_init=True)
+    monkeypatch.setenv("EVP1D_COMPACT", "0")
+    assert not roofline.short_stepu(pr, 0.0)

@@ -300,6 +300,46 @@ def test_nonfinite_inputs(oracle_mod):
     assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 5), pr)
 
 
+@pytest.mark.parametrize("case", ["signed_zeros", "tbu_minus_zero", "tbu_nonzero",
+                                  "uinit_inf", "revp_minus_zero", "compact_off"])
+def test_short_stepu_part_edges(oracle_mod, monkeypatch, case):
+    """The subcycle kernel copies a stepu part without Tbu, uinit and vinit
+    when every Tbu of the call is +0 and every uinit, vinit is finite (with
+    revp == 0): Tbu is then +0 and revp*uinit a zero with uinit's sign.
+    Explicit uvel_init/vvel_init of both signs and signed zeros, velocities
+    that are -0 (so brlx*uold + revp*uinit is a sum of two zeros), revp = -0,
+    and fields that rule the short part out (Tbu = -0 or 1e-3 at one point,
+    an infinite uinit): every case gives the oracle's bits."""
+    if case == "compact_off":
+        monkeypatch.setenv("EVP1D_COMPACT", "0")
+    pr = synth.make_problem("grid400x300", nx=64, ny=40, seed=29, ndte=6)
+    rng = np.random.default_rng(33)
+    n = pr.na
+    ui = rng.normal(0, 0.05, n)
+    vi = rng.normal(0, 0.05, n)
+    z = rng.random(n)
+    ui = np.where(z < 0.1, 0.0, np.where(z < 0.2, -0.0, ui))
+    vi = np.where(z > 0.9, -0.0, np.where(z > 0.8, 0.0, vi))
+    pr.f["uvel_init"], pr.f["vvel_init"] = ui, vi
+    w = rng.random(n)
+    pr.uvel[:n] = np.where(w < 0.15, -0.0, pr.uvel[:n])
+    pr.vvel[:n] = np.where(w > 0.85, -0.0, pr.vvel[:n])
+    p = evp1d.set_evp_parameters(6)
+    if case == "revp_minus_zero":
+        p.revp = -0.0
+    k = n // 3
+    if case == "tbu_minus_zero":
+        pr.f["Tbu"] = pr.f["Tbu"].copy()
+        pr.f["Tbu"][k] = -0.0
+    elif case == "tbu_nonzero":
+        pr.f["Tbu"] = pr.f["Tbu"].copy()
+        pr.f["Tbu"][k] = 1e-3
+    elif case == "uinit_inf":
+        pr.f["uvel_init"][k] = np.inf
+    fs = gpu_run(pr, 6, params=p, explicit_init=True)
+    assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 6, params=p), pr)
+
+
 @pytest.mark.parametrize("points", [128, 200])
 def test_smaller_tiles_bitwise(oracle_mod, points):
     """Plans with a smaller largest tile (evp1d_set_tile_points) give the same
