@@ -313,6 +313,7 @@ int init_common(evp1d_t **handle, int na, int navel, const int32_t *const idx[6]
   if (const char *e = getenv("EVP1D_PERSIST"))
     h->persist = atoi(e) != 0 && evp::tma_can_persist(device, plan.nruns);
   if (const char *e = getenv("EVP1D_PDL")) h->pdl = atoi(e) != 0;
+  if (const char *e = getenv("EVP1D_COMPACT")) h->d.compact_allowed = atoi(e) != 0;
   *handle = h;
   return EVP1D_OK;
 }

@@ -72,6 +72,7 @@ struct DeviceProblem {
   // device word of launch_const_blocks' field checks: 0 when every Tbu of the
   // call is +0 and every uinit, vinit finite (TmaArgs::compact)
   int *cflags = nullptr;
+  bool compact_allowed = true;  // EVP1D_COMPACT=0 at init turns the short part off
   int nctas = 0;             // SM count of the device
   uint8_t *flags = nullptr;
   double *geo[kNumGeo] = {};

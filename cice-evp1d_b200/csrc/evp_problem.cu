@@ -1,6 +1,5 @@
 // evp_problem.cu -- device arena of one 1D problem and its movement between
 // the caller's reference-order host arrays and the slot-ordered device state.
-#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -491,14 +490,7 @@ TmaArgs problem_tma_args(const DeviceProblem &d, int from) {
   a.sg[6] = d.dyn[kStrength];
   a.cblk = d.cblk;
   a.cflags = d.cflags;
-  // the short stepu part where the call's fields allow it (EVP1D_COMPACT=0: never)
-  {
-    static const bool allowed = [] {
-      const char *e = getenv("EVP1D_COMPACT");
-      return !(e && atoi(e) == 0);
-    }();
-    a.compact = allowed;
-  }
+  a.compact = d.compact_allowed;
   a.u[0] = d.u[from];
   a.v[0] = d.v[from];
   a.u[1] = d.u[to];
