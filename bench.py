@@ -1244,8 +1244,8 @@ def main():
     solver.finalize()
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
-        extras["ensemble"] = ensemble_extras(local, 2, args.extras_ndte)
-        extras["adjoint"] = adjoint_extras(local, 2, args.extras_ndte)
+        extras["ensemble"] = ensemble_extras(local, 3, args.extras_ndte)
+        extras["adjoint"] = adjoint_extras(local, 3, args.extras_ndte)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,

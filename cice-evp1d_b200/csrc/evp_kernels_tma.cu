@@ -25,7 +25,9 @@
 // stepu still reads the two before it.  The 13 stepu inputs of a tile (the
 // second part of its constant block) arrive by one more bulk copy into a
 // stepu slot, which the consumers release as soon as each has its point's
-// inputs in registers.
+// inputs in registers.  Where every Tbu of the call is +0, every uinit and
+// vinit finite and revp == 0, the part stops after its tenth field: Tbu is
+// +0, and revp*uinit a signed zero whose sign comes from the packed word.
 // Consecutive one-subcycle launches overlap: each CTA lets the next launch
 // start at once (griddepcontrol.launch_dependents), and a launch started that
 // way loads its first tile's records, constants and stepu part while the
