@@ -1262,6 +1262,12 @@ def main():
                          "kernel": path,
                          "stepu_part": ("short: Tbu +0, uvel_init/vvel_init finite, revp 0"
                                         if short else "full"),
+                         # the same rate over the full stepu part's 401 B, for
+                         # comparison with calls that need it
+                         "full_part_equivalent": {
+                             "bytes_per_point_subcycle": alg_bytes.per_point_subcycle(path),
+                             "equivalent_gbs": alg_bytes.per_point_subcycle(path) * pr.n_active / sub_s / 1e9,
+                             "equivalent_frac": alg_bytes.per_point_subcycle(path) * pr.n_active / sub_s / 1e9 / peak},
                          # the same rate over the reference's unfused data
                          # contract (str1..8 through HBM, 576 B): what the
                          # reference's two kernels would have to move
