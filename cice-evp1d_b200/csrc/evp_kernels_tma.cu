@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
           }
         }
         w = __shfl_sync(0xffffffffu, w, 0);
-        if (w && multi && sub > 0) {
+        if constexpr (kMulti) if (w && sub > 0) {
           // the tiles step q depends on have finished subcycle sub - 1; the
           // warp waits together, lane 0 publishing this CTA's finished steps
           // meanwhile (a tile may wait on its own run's steps)
