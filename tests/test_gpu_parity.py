@@ -340,6 +340,29 @@ def test_short_stepu_part_edges(oracle_mod, monkeypatch, case):
     assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 6, params=p), pr)
 
 
+def test_concurrent_handles_bitwise(oracle_mod):
+    """Three handles on their own streams, their calls issued back to back
+    without waiting (each call's subcycle launches overlap the launch before
+    them on the same stream, and the streams run side by side): every
+    handle's results are the oracle's bits."""
+    probs = [synth.to_1d(synth.make_grid(nx, ny, seed=70 + i, ndte=120, curvilinear=True))
+             for i, (nx, ny) in enumerate([(90, 70), (150, 110), (60, 40)])]
+    handles = [evp1d.EVP1D.from_problem(pr, ndte=120) for pr in probs]
+    try:
+        sets = [evp1d.FieldSet.from_problem(pr) for pr in probs]
+        for h, fs in zip(handles, sets):
+            h.upload(fs)
+        for h in handles:
+            h.subcycles(120)
+        for h, fs in zip(handles, sets):
+            h.download(fs)
+    finally:
+        for h in handles:
+            h.finalize()
+    for pr, fs in zip(probs, sets):
+        assert_same(fs, oracle_run(oracle_mod, pr, 120), pr, check_str=False)
+
+
 @pytest.mark.parametrize("points", [128, 200])
 def test_smaller_tiles_bitwise(oracle_mod, points):
     """Plans with a smaller largest tile (evp1d_set_tile_points) give the same
