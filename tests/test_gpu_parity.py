@@ -433,11 +433,16 @@ def test_golden_fixture_md5():
     assert np.array_equal(fs.str.view(np.int64), out["str"].view(np.int64))
 
 
-def test_batched_ensemble_matches_members(oracle_mod):
+@pytest.mark.parametrize("tbu_member", [None, 3])
+def test_batched_ensemble_matches_members(oracle_mod, tbu_member):
     """Uneven members solved in one handle give, member by member, bitwise the
-    single-member results (and the oracle's)."""
+    single-member results (and the oracle's); with basal stress in one
+    member, the whole batch takes the full stepu part."""
     members = [synth.make_problem("grid400x300", nx=nx, ny=ny, seed=40 + i, ndte=8)
                for i, (nx, ny) in enumerate([(30, 20), (75, 41), (12, 9), (50, 60), (90, 17)])]
+    if tbu_member is not None:
+        m = members[tbu_member]
+        m.f["Tbu"] = np.random.default_rng(7).uniform(0.0, 5.0, m.na)
     ens = synth.concat(members)
     fs = evp1d.FieldSet.from_problem(ens.combined, want_str=True)
     with evp1d.EVP1D.batched(ens, ndte=8) as s:
