@@ -406,32 +406,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
           }
         }
         w = __shfl_sync(0xffffffffu, w, 0);
-        if constexpr (kMulti) if (w && sub > 0) {
-          // the tiles step q depends on have finished subcycle sub - 1; the
-          // warp waits together, lane 0 publishing this CTA's finished steps
-          // meanwhile (a tile may wait on its own run's steps)
-          const unsigned need = (unsigned)sub;
-          const int d0 = a.dep_off[t], d1 = a.dep_off[t + 1];
-          const unsigned long long t0 = global_ns();
-          for (bool first = true;; first = false) {
-            bool mine = true;
-            for (int d = d0 + lane; d < d1 && mine; d += 32) {
-              if (first && d < d0 + 32 && seen >= need) continue;
-              mine = ld_relaxed(a.epoch + a.dep_idx[d]) >= need;
+        if constexpr (kMulti) {
+          if (w && sub > 0) {
+            // the tiles step q depends on have finished subcycle sub - 1; the
+            // warp waits together, lane 0 publishing this CTA's finished steps
+            // meanwhile (a tile may wait on its own run's steps)
+            const unsigned need = (unsigned)sub;
+            const int d0 = a.dep_off[t], d1 = a.dep_off[t + 1];
+            const unsigned long long t0 = global_ns();
+            for (bool first = true;; first = false) {
+              bool mine = true;
+              for (int d = d0 + lane; d < d1 && mine; d += 32) {
+                if (first && d < d0 + 32 && seen >= need) continue;
+                mine = ld_relaxed(a.epoch + a.dep_idx[d]) >= need;
+              }
+              if (__all_sync(0xffffffffu, mine)) break;
+              if (lane == 0) publish(q);
+              // one decision for the whole warp (lane 0's clock)
+              if (__shfl_sync(0xffffffffu, global_ns() - t0 > kWaitNs ? 1 : 0, 0)) {
+                if (lane == 0) atomicMax(a.err, 13);
+                w = 0;
+                break;
+              }
             }
-            if (__all_sync(0xffffffffu, mine)) break;
-            if (lane == 0) publish(q);
-            // one decision for the whole warp (lane 0's clock)
-            if (__shfl_sync(0xffffffffu, global_ns() - t0 > kWaitNs ? 1 : 0, 0)) {
-              if (lane == 0) atomicMax(a.err, 13);
-              w = 0;
-              break;
-            }
+            // acquire: the neighbours' state is read after their counters, by
+            // these bulk copies (async proxy) and by the gather warps
+            fence_acq_rel_gpu();
+            fence_proxy_async_global();
           }
-          // acquire: the neighbours' state is read after their counters, by
-          // these bulk copies (async proxy) and by the gather warps
-          fence_acq_rel_gpu();
-          fence_proxy_async_global();
         }
         if (lane == 0) trace_stamp(a, issued, 4);
         if (w) {
