@@ -85,6 +85,10 @@ struct AdjArgs {
 
 // lam of u(n+1), v(n+1) at x: stepu's own part plus the stress corners that
 // read the velocity at x (as cc of x, and as ee/ne/se of other T points).
+// With one entry per transposed list (kOne) each U point has at most one
+// such T point per role, and k_adj_stress stores that corner's share at the
+// U point's own slot (C8[2..7] indexed by x; slots no T point writes keep the
+// zeros of the seed): the sum reads x's slots straight, with no index.
 template <bool kOne>
 __device__ __forceinline__ void velocity_lam(const AdjArgs &a, int x, double &lu,
                                              double &lv) {
@@ -93,11 +97,8 @@ __device__ __forceinline__ void velocity_lam(const AdjArgs &a, int x, double &lu
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     if (kOne) {
-      const int w = a.tr_one[kTrEe + k][x];
-      if (w >= 0) {
-        lu += a.C8[2 + 2 * k][w];
-        lv += a.C8[3 + 2 * k][w];
-      }
+      lu += a.C8[2 + 2 * k][x];
+      lv += a.C8[3 + 2 * k][x];
     } else {
       const int32_t *off = a.tr_off[kTrEe + k], *idx = a.tr_idx[kTrEe + k];
       const int b = off[x], e = off[x + 1];
@@ -182,6 +183,29 @@ k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__
   }
 }
 
+// The 8 corner velocity adjoints of T point w: cc at w's slot; ee, ne, se at
+// w's slot (read back through the transposed lists), or with kOne at the
+// slots of those U points (velocity_lam), halo slots having no U point.
+template <bool kOne>
+__device__ __forceinline__ void store_corners(const AdjArgs &a, int w, int iee, int ine, int ise,
+                                              const double (&lc)[8]) {
+  a.C8[0][w] = lc[0];
+  a.C8[1][w] = lc[1];
+  if (kOne) {
+    const int t[3] = {iee, ine, ise};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      if (t[k] < a.nslots) {
+        a.C8[2 + 2 * k][t[k]] = lc[2 + 2 * k];
+        a.C8[3 + 2 * k][t[k]] = lc[3 + 2 * k];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 2; k < 8; k++) a.C8[k][w] = lc[k];
+  }
+}
+
 template <bool kOne>
 __global__ void __launch_bounds__(kThreads, 2)
 k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__restrict__ v) {
@@ -189,9 +213,10 @@ k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__
   griddep_wait();
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < a.nslots;
        w += gridDim.x * blockDim.x) {
+    const int iee = a.ee[w], ine = a.ne[w], ise = a.se[w];
     if (a.flags[w] & kSkipT) {  // stresses unchanged, str not written
-#pragma unroll
-      for (int k = 0; k < 8; k++) a.C8[k][w] = 0.0;
+      double zero[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      store_corners<kOne>(a, w, iee, ine, ise, zero);
       continue;
     }
     double lo[8];
@@ -203,7 +228,6 @@ k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__
     double ls[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) ls[k] = a.LS[k][w];
-    const int iee = a.ee[w], ine = a.ne[w], ise = a.se[w];
     Corners c;
     c.ucc = u[w];
     c.vcc = v[w];
@@ -219,8 +243,7 @@ k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__
     stress_adjoint(c, g, a.strength[w], p, lo, ls, lc, lstr);
 #pragma unroll
     for (int k = 0; k < 12; k++) a.LS[k][w] = ls[k];
-#pragma unroll
-    for (int k = 0; k < 8; k++) a.C8[k][w] = lc[k];
+    store_corners<kOne>(a, w, iee, ine, ise, lc);
     a.g[kGStrength][w] += lstr;
   }
 }
