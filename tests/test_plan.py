@@ -103,6 +103,18 @@ def test_plan_check_passes_on_grids(points):
         evp1d.set_tile_points(old)
 
 
+def test_plan_check_passes_on_a_large_grid():
+    """4.4 M points (3000 x 2400, 17,619 tiles, runs of up to 120 tiles):
+    every packed index and range still decodes to what the neighbour
+    vectors say, and the caps hold."""
+    pr = synth.to_1d(synth.make_grid(3000, 2400, seed=5, ndte=2))
+    st = stats(pr)
+    assert pr.na > 4_000_000 and st["from_coords"]
+    assert st["max_tile"] <= TILE and st["max_halo"] <= 64 and st["max_extras"] <= 128
+    assert st["halo"] < 0.02 * pr.na
+    evp1d.plan_check(pr.na, pr.navel, pr.idx)
+
+
 def test_plan_check_passes_on_the_reference_shaped_problems():
     _check(synth.make_problem("grid400x300"))
     _check(helpers.standalone_problem())
