@@ -1,5 +1,6 @@
-"""The bench's full-size workload (1600 x 1200 grid, 1,180,692 points, 4660
-tiles: every SM cycles its shared-memory slots and record ring many times).
+"""The bench's full-size workload (1600 x 1200 grid, 1,180,692 points, 4726
+tiles: every SM cycles its shared-memory slots and record ring many times),
+and a larger grid (3000 x 2400, 4.4 M points, runs of up to 120 tiles).
 
 - Three subcycles against the oracle, bit for bit, with md5-equal output
   files (src/vars.F90:2233-2304).
@@ -10,6 +11,8 @@ tiles: every SM cycles its shared-memory slots and record ring many times).
   does not enter the update, so nothing else depends on where a call starts.
   The 1000-subcycle call also runs the captured-graph chunks end to end.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -49,3 +52,14 @@ def test_grid1600x1200_two_calls_of_500_equal_one_of_1000(big):
         assert np.array_equal(np.asarray(a).view(np.int64), np.asarray(b).view(np.int64)), name
     # the state moved: the property is not trivially met by an idle solver
     assert not np.array_equal(one.uvel[:na], pr.uvel[:na])
+
+
+def test_grid3000x2400_sixty_subcycles_bitwise(oracle_mod):
+    """4.4 M points, 17,619 tiles in runs of up to 120, 60 subcycles (one
+    captured chunk of 50 and ten launches after it): every output bit for
+    bit against the oracle's OpenMP run."""
+    pr = synth.to_1d(synth.make_grid(3000, 2400, seed=5, ndte=60))
+    assert pr.na > 4_000_000
+    fs = gpu_run(pr, 60, want_str=False)
+    st = oracle_mod.run_1d(pr, 60, mode="omp", nthreads=os.cpu_count() or 1)
+    assert_same(fs, st, pr, check_str=False)
