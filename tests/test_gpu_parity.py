@@ -340,6 +340,26 @@ def test_short_stepu_part_edges(oracle_mod, monkeypatch, case):
     assert_same_nan_aware(fs, oracle_run(oracle_mod, pr, 6, params=p), pr)
 
 
+def test_params_change_between_calls_bitwise(oracle_mod):
+    """One handle runs a call with the default parameters (revp = 0, Tbu = 0:
+    the short stepu part, captured in graphs), then, after evp1d_set_params,
+    a call with revised EVP (revp = 1), whose stepu needs uvel_init; then the
+    defaults again.  Each call gives the oracle's bits for its parameters."""
+    pr = synth.to_1d(synth.make_grid(120, 90, seed=81, ndte=120, curvilinear=True))
+    rng = np.random.default_rng(8)
+    pr.f["uvel_init"] = pr.f["uvel_init"] + rng.normal(0, 0.01, pr.na)
+    p0 = evp1d.set_evp_parameters(120)
+    p1 = evp1d.set_evp_parameters(120)
+    p1.revp = 1.0
+    with evp1d.EVP1D.from_problem(pr, ndte=120, params=p0) as s:
+        for p in (p0, p1, p0):
+            s.set_params(p)
+            # uvel_init given explicitly, as the oracle reads it from the fields
+            fs = evp1d.FieldSet.from_problem(pr, explicit_init=True)
+            s.run(120, fs)
+            assert_same(fs, oracle_run(oracle_mod, pr, 120, params=p), pr, check_str=False)
+
+
 def test_concurrent_handles_bitwise(oracle_mod):
     """Three handles on their own streams, their calls issued back to back
     without waiting (each call's subcycle launches overlap the launch before
