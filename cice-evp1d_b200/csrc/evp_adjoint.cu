@@ -133,7 +133,7 @@ __device__ __forceinline__ void str_lam(const AdjArgs &a, int t, int w, double &
 }
 
 template <bool kOne>
-__global__ void __launch_bounds__(kThreads, 4)  // 64 registers: 32 warps per SM
+__global__ void __launch_bounds__(kThreads, 3)  // 80 registers: 24 warps per SM, no spills
 k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__restrict__ v0,
             const double *__restrict__ u1, const double *__restrict__ v1) {
   // launched as a programmatic dependent: the previous kernel's results
@@ -142,15 +142,11 @@ k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__
   griddep_wait();
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.nslots;
        x += gridDim.x * blockDim.x) {
+    // Every input is loaded before the skip test (all arrays hold nslots
+    // entries), so the loads go out in one round instead of two.
     double lu, lv;
     velocity_lam<kOne>(a, x, lu, lv);
-    if (a.flags[x] & kSkipU) {  // u(n+1) = u(n) here
-      a.Pu[x] = lu;
-      a.Pv[x] = lv;
-      a.Lx[x] = 0.0;
-      a.Ly[x] = 0.0;
-      continue;
-    }
+    const bool skip = a.flags[x] & kSkipU;
     StepuAdjIn in;
     in.uold = u0[x];
     in.vold = v0[x];
@@ -167,16 +163,19 @@ k_adj_stepu(AdjArgs a, Params p, const double *__restrict__ u0, const double *__
     in.umassdti = a.umassdti[x];
     in.fm = a.fm[x];
     in.Tbu = a.Tbu[x];
-    const StepuAdjOut o = stepu_adjoint(in, p);
-    a.Pu[x] = o.luold;
-    a.Pv[x] = o.lvold;
     const double ar = a.uarear[x];
-    a.Lx[x] = ar * o.lcc1;
-    a.Ly[x] = ar * o.lcc2;
-    a.g[kGForcex][x] += o.lcc1;
-    a.g[kGForcey][x] += o.lcc2;
-    a.g[kGCw][x] += o.gCw;
-    if (p.revp != 0.0) {
+    const double gfx = a.g[kGForcex][x], gfy = a.g[kGForcey][x], gcw = a.g[kGCw][x];
+    // a skipped point (u(n+1) = u(n) there) passes lam on unchanged and
+    // takes no gradient; selects, not branches, keep the loads above
+    const StepuAdjOut o = stepu_adjoint(in, p);
+    a.Pu[x] = skip ? lu : o.luold;
+    a.Pv[x] = skip ? lv : o.lvold;
+    a.Lx[x] = skip ? 0.0 : ar * o.lcc1;
+    a.Ly[x] = skip ? 0.0 : ar * o.lcc2;
+    a.g[kGForcex][x] = skip ? gfx : gfx + o.lcc1;
+    a.g[kGForcey][x] = skip ? gfy : gfy + o.lcc2;
+    a.g[kGCw][x] = skip ? gcw : gcw + o.gCw;
+    if (p.revp != 0.0 && !skip) {
       a.g[kGUinit][x] += o.luinit;
       a.g[kGVinit][x] += o.lvinit;
     }
@@ -237,7 +236,7 @@ k_adj_stress(AdjArgs a, Params p, const double *__restrict__ u, const double *__
     c.vne = v[ine];
     c.use = u[ise];
     c.vse = v[ise];
-    const Geom g = make_geom(a.dxT[w], a.dyT[w], a.HTE[w], a.HTN[w], a.HTEm1[w],
+    const Geom g = make_geom_fw(a.dxT[w], a.dyT[w], a.HTE[w], a.HTN[w], a.HTEm1[w],
                              a.HTNm1[w], p.deltaminEVP);
     double lc[8], lstr;
     stress_adjoint(c, g, a.strength[w], p, lo, ls, lc, lstr);
@@ -268,16 +267,34 @@ __global__ void __launch_bounds__(kThreads) k_adj_final(AdjArgs a, int fold_init
 // The forward kernels write u, v only at the slots they update (U points that
 // are not skipU); the ping-pong buffers keep the constant rest.  Tape entries
 // get that constant part -- skipU and padding slots [0, nslots) and halo
-// slots [nslots, nuv) -- from src, for entries 1..count-1 of a tape whose
-// entries are `stride` doubles apart.
-__global__ void k_fill_constant(double *tape, size_t stride, int nslots, int nuv,
-                                int count, const double *src, const uint8_t *flags) {
-  const long long total = (long long)nuv * (count - 1);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int e = 1 + (int)(t / nuv), j = (int)(t % nuv);
-    if (j >= nslots || (flags[j] & kSkipU)) tape[(size_t)e * stride + j] = src[j];
-  }
+// slots [nslots, nuv) -- from su (blockIdx.y 0) and sv (1), for entries
+// 1..count-1 of a tape whose entries are `entry_step` doubles apart, v at
+// v_off after u.  One thread per slot: a slot the kernels update returns at
+// once, a constant one reads its value once and stores it into every entry.
+__global__ void k_fill_constant(double *tape, size_t entry_step, size_t v_off, int nslots,
+                                int nuv, int count, const double *su, const double *sv,
+                                const uint8_t *flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nuv || (j < nslots && !(flags[j] & kSkipU))) return;
+  const double x = (blockIdx.y ? sv : su)[j];
+  double *t = tape + (blockIdx.y ? v_off : 0) + j;
+  for (int e = 1; e < count; e++) t[(size_t)e * entry_step] = x;
+}
+
+// One checkpoint's state: u, v (nuv doubles each) and the 12 stresses
+// (nslots each), array blockIdx.y, copied in one launch.
+struct StateCopy {
+  const double *src[14];
+  double *dst[14];
+};
+
+__global__ void k_copy_state(StateCopy c, int nuv, int nslots) {
+  const int q = blockIdx.y;
+  const int n = q < 2 ? nuv : nslots;
+  const double *__restrict__ src = c.src[q];
+  double *__restrict__ dst = c.dst[q];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[i] = src[i];
 }
 
 int blocks_for(long long n) {
@@ -653,23 +670,26 @@ int evp1d_record_subcycles(evp1d_t *h, int ndte, int interval) {
   const int cur0 = d.cur;
   // the constant slots of every tape entry (entry 0 is copied whole each time)
   if (entries > 1) {
-    const long long work = (long long)d.nuv * (entries - 1);
-    k_fill_constant<<<blocks_for(work), kThreads, 0, st>>>(
-        A.tape, 2 * A.stride, d.nslots, d.nuv, entries, d.u[cur0], d.flags);
-    k_fill_constant<<<blocks_for(work), kThreads, 0, st>>>(
-        A.tape + A.stride, 2 * A.stride, d.nslots, d.nuv, entries, d.v[cur0], d.flags);
+    const dim3 grid((unsigned)((d.nuv + kThreads - 1) / kThreads), 2);
+    k_fill_constant<<<grid, kThreads, 0, st>>>(A.tape, 2 * A.stride, A.stride, d.nslots, d.nuv,
+                                               entries, d.u[cur0], d.v[cur0], d.flags);
+    h->launches++;
   }
   // checkpointed head: the ordinary subcycle loop with a copy of the state
   // at the start of every segment
   for (int j = 0; j < nck; j++) {
     const int c = d.cur;
-    ADJ_TRY(cudaMemcpyAsync(ck_u(A, j), d.u[c], sizeof(double) * d.nuv,
-                            cudaMemcpyDeviceToDevice, st));
-    ADJ_TRY(cudaMemcpyAsync(ck_v(A, j), d.v[c], sizeof(double) * d.nuv,
-                            cudaMemcpyDeviceToDevice, st));
-    for (int q = 0; q < 12; q++)
-      ADJ_TRY(cudaMemcpyAsync(ck_s(A, j, q), d.stress[c][q], sizeof(double) * d.nslots,
-                              cudaMemcpyDeviceToDevice, st));
+    StateCopy cp;
+    cp.src[0] = d.u[c];
+    cp.src[1] = d.v[c];
+    cp.dst[0] = ck_u(A, j);
+    cp.dst[1] = ck_v(A, j);
+    for (int q = 0; q < 12; q++) {
+      cp.src[2 + q] = d.stress[c][q];
+      cp.dst[2 + q] = ck_s(A, j, q);
+    }
+    k_copy_state<<<dim3(blocks_for(d.nuv), 14), kThreads, 0, st>>>(cp, d.nuv, d.nslots);
+    h->launches++;
     ADJ_CHECK(evp1d_subcycles(h, std::min(k, n_cp - j * k)));
   }
   // taped tail: each subcycle writes its velocities into the next entry
@@ -799,19 +819,37 @@ int evp1d_adjoint_sweep(evp1d_t *h) {
   const int k = A.interval;
   for (int j = A.nck - 1; j >= 0; j--) {
     const int len = std::min(k, A.n_cp - j * k);
-    ADJ_TRY(cudaMemcpyAsync(tape_u(A, A.seg_base), ck_u(A, j), sizeof(double) * d.nuv,
-                            cudaMemcpyDeviceToDevice, st));
-    ADJ_TRY(cudaMemcpyAsync(tape_v(A, A.seg_base), ck_v(A, j), sizeof(double) * d.nuv,
-                            cudaMemcpyDeviceToDevice, st));
-    for (int q = 0; q < 12; q++)
-      ADJ_TRY(cudaMemcpyAsync(A.spp[0][q], ck_s(A, j, q), sizeof(double) * d.nslots,
-                              cudaMemcpyDeviceToDevice, st));
-    // recompute the segment's velocities from its checkpoint
     const int e0 = A.seg_base;
+    StateCopy cp;
+    cp.src[0] = ck_u(A, j);
+    cp.src[1] = ck_v(A, j);
+    cp.dst[0] = tape_u(A, e0);
+    cp.dst[1] = tape_v(A, e0);
+    for (int q = 0; q < 12; q++) {
+      cp.src[2 + q] = ck_s(A, j, q);
+      cp.dst[2 + q] = A.spp[0][q];
+    }
+    k_copy_state<<<dim3(blocks_for(d.nuv), 14), kThreads, 0, st>>>(cp, d.nuv, d.nslots);
+    launches++;
+    // Recompute the segment's velocities from its checkpoint.  Its end state
+    // is stored already -- the next checkpoint's u, v, or the taped tail's
+    // first entry -- so the last subcycle is copied, not recomputed (the
+    // forward is deterministic: the same bits).
+    const bool end_stored = j + 1 < A.nck || A.n_cp < A.ndte;
+    const int nrec = end_stored ? len - 1 : len;
     const long long before = h->launches;
-    launch_states(h, A.spp[0], A.spp[1], tape_u(A, e0), tape_v(A, e0), 2 * A.stride, len, false);
+    launch_states(h, A.spp[0], A.spp[1], tape_u(A, e0), tape_v(A, e0), 2 * A.stride, nrec,
+                  false);
     launches += h->launches - before;
     h->launches = before;
+    if (end_stored) {
+      const double *eu = j + 1 < A.nck ? ck_u(A, j + 1) : tape_u(A, 0);
+      const double *ev = j + 1 < A.nck ? ck_v(A, j + 1) : tape_v(A, 0);
+      ADJ_TRY(cudaMemcpyAsync(tape_u(A, e0 + len), eu, sizeof(double) * d.nuv,
+                              cudaMemcpyDeviceToDevice, st));
+      ADJ_TRY(cudaMemcpyAsync(tape_v(A, e0 + len), ev, sizeof(double) * d.nuv,
+                              cudaMemcpyDeviceToDevice, st));
+    }
     for (int i = len - 1; i >= 0; i--)
       reverse_step(tape_u(A, e0 + i), tape_v(A, e0 + i), tape_u(A, e0 + i + 1),
                    tape_v(A, e0 + i + 1));

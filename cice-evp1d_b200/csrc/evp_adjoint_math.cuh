@@ -2,7 +2,8 @@
 // point (hand-written, FP64).
 //
 // The forward quantities a derivative needs are recomputed from the stored
-// velocities with the forward's own functions (evp_math.cuh), so every branch
+// velocities in the forward's own operation order (evp_math.cuh; the
+// branch-deciding ones below with the forward's rounding), so every branch
 // takes the side the forward took: max(Delta, DminArea) (src/bench_v2b.F90:
 // 428-430), the capped/uncapped viscosity, and a zero-length square root
 // (Delta = 0, |u| = 0, |u_ocn - u| = 0), whose derivative is taken as 0.
@@ -11,12 +12,84 @@
 // relaxation is linear in the old stresses with state-independent
 // coefficients, so the reverse sweep needs the velocities of each subcycle
 // but never the stresses.  These derivatives are not bit-matched to anything:
-// a reciprocal is multiplied where the forward divides.
+// a reciprocal is multiplied where the forward divides, and the reverse
+// kernels are compiled with a*b+c contracted to fused multiply-adds.
+//
+// The forward values that choose a branch -- Delta against DminTarea and 0,
+// |u| and |u_ocn - u| against 0 -- are recomputed with every +, -, * rounded
+// on its own (fw_mul/fw_add/fw_sub: the __d*_rn intrinsics, which the
+// compiler never contracts), in the forward's operation order, so they equal
+// the bit-exact forward's values whatever the file's contraction setting.
+// In the FMA flavour of the library (EVP_FMA) the forward itself is
+// contracted, so these are plain operations there as well.
 #pragma once
 
 #include "evp_math.cuh"
 
 namespace evp {
+
+__host__ __device__ __forceinline__ double fw_mul(double a, double b) {
+#if defined(__CUDA_ARCH__) && !defined(EVP_FMA)
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ double fw_add(double a, double b) {
+#if defined(__CUDA_ARCH__) && !defined(EVP_FMA)
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+__host__ __device__ __forceinline__ double fw_sub(double a, double b) {
+#if defined(__CUDA_ARCH__) && !defined(EVP_FMA)
+  return __dsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
+
+// make_geom (src/bench_v2b.F90:137-147) with every operation rounded on its
+// own: the same bits as the forward's geometry.
+__host__ __device__ __forceinline__ Geom make_geom_fw(double dxT, double dyT, double hte,
+                                                      double htn, double htem1, double htnm1,
+                                                      double deltaminEVP) {
+  Geom g;
+  g.dxT = dxT;
+  g.dyT = dyT;
+  g.cxp = fw_sub(fw_mul(kC1p5, htn), fw_mul(kP5, htnm1));
+  g.cyp = fw_sub(fw_mul(kC1p5, hte), fw_mul(kP5, htem1));
+  g.cxm = -fw_sub(fw_mul(kC1p5, htnm1), fw_mul(kP5, htn));
+  g.cym = -fw_sub(fw_mul(kC1p5, htem1), fw_mul(kP5, hte));
+  g.DminTarea = fw_mul(deltaminEVP, fw_mul(dxT, dyT));
+  g.dxhy = fw_mul(kP5, fw_sub(hte, htem1));
+  g.dyhx = fw_mul(kP5, fw_sub(htn, htnm1));
+  return g;
+}
+
+// corner_strain (the strain rates and Delta of one corner, src/bench_v2b.F90:
+// 363-397) with every operation rounded on its own, left to right as in the
+// forward: the same div, ten, shr and Delta bits.
+__host__ __device__ __forceinline__ void corner_strain_fw(
+    int k, double u1, double v1, double u2, double v2, double u4, double v4, const Geom &g,
+    double e_factor, double &div, double &ten, double &shr, double &Delta) {
+  const bool a = (k == 0) | (k == 3);
+  const bool b = k < 2;
+  const double A1 = a ? g.cyp : g.cym;
+  const double C1 = a ? g.cym : g.cyp;
+  const double A3 = b ? g.cxp : g.cxm;
+  const double C3 = b ? g.cxm : g.cxp;
+  const double B2 = a ? -g.dyT : g.dyT;
+  const double B4 = b ? -g.dxT : g.dxT;
+  div = fw_add(fw_add(fw_add(fw_mul(A1, u1), fw_mul(B2, u2)), fw_mul(A3, v1)), fw_mul(B4, v4));
+  ten = fw_add(fw_add(fw_add(-fw_mul(C1, u1), fw_mul(B2, u2)), fw_mul(C3, v1)),
+               fw_mul(-B4, v4));
+  shr = fw_add(fw_add(fw_add(-fw_mul(C1, v1), fw_mul(B2, v2)), fw_mul(-C3, u1)),
+               fw_mul(B4, u4));
+  Delta = sqrt(fw_add(fw_mul(div, div),
+                      fw_mul(e_factor, fw_add(fw_mul(ten, ten), fw_mul(shr, shr)))));
+}
 
 // Transpose of str_combine (src/bench_v2b.F90:217-310): given lo[0..7] =
 // dJ/d str1..str8 at a point, add dJ/d s[0..11] (the updated stresses) to ls.
@@ -126,8 +199,9 @@ __host__ __device__ __forceinline__ void corner_adjoint(
 // lam of the old stresses).  Returns the lam of the 8 corner velocities and
 // the point's dJ/dstrength contribution.
 //
-// Corner by corner: corner_strain gives the corner's div, ten, shr and Delta
-// (bit for bit those of strain_rates, so every branch follows the forward),
+// Corner by corner: corner_strain_fw gives the corner's div, ten, shr and
+// Delta (bit for bit those of strain_rates, so every branch follows the
+// forward; g must come from make_geom_fw),
 // corner_adjoint reverses its relaxation, and the corner's share of the
 // transposed strain rates is added to lc at once.  Only one corner's strain
 // is live at a time.  With P1 = (cc, ee, ne, se)[k], P2 = (ee, cc, se, ne)[k],
@@ -150,8 +224,8 @@ __host__ __device__ __forceinline__ void stress_adjoint(const Corners &c, const 
   for (int k = 0; k < 4; k++) {
     const int p1 = k, p2 = k ^ 1, p4 = 3 - k;
     double div, ten, shr, Delta;
-    corner_strain(k, uu[p1], vv[p1], uu[p2], vv[p2], uu[p4], vv[p4], g, p.e_factor, div, ten,
-                  shr, Delta);
+    corner_strain_fw(k, uu[p1], vv[p1], uu[p2], vv[p2], uu[p4], vv[p4], g, p.e_factor, div,
+                     ten, shr, Delta);
     double D, T, H, lst;
     corner_adjoint(ls[k], ls[4 + k], ls[8 + k], div, ten, shr, Delta, strength, g.DminTarea, p,
                    D, T, H, lst);
@@ -193,10 +267,11 @@ __host__ __device__ __forceinline__ StepuAdjOut stepu_adjoint(const StepuAdjIn &
                                                               const Params &p) {
   StepuAdjOut o;
   const double u = in.uold, v = in.vold;
-  const double du = in.uocn - u, dv = in.vocn - v;
-  const double sq = sqrt(du * du + dv * dv);
+  // |u_ocn - u| and |u| as the forward rounds them (they are tested against 0)
+  const double du = fw_sub(in.uocn, u), dv = fw_sub(in.vocn, v);
+  const double sq = sqrt(fw_add(fw_mul(du, du), fw_mul(dv, dv)));
   const double vrel = in.kvrel * sq;
-  const double sn = sqrt(u * u + v * v);
+  const double sn = sqrt(fw_add(fw_mul(u, u), fw_mul(v, v)));
   const double den = sn + p.u0;
   const double Cb = in.Tbu / den;
   const double cca = (p.brlx + p.revp) * in.umassdti + vrel * p.cosw + Cb;

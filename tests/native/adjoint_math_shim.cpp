@@ -44,7 +44,7 @@ void shim_stress_adjoint(int n, const double *corners, const double *geo,
     c.vne = corners[5 * n + w];
     c.use = corners[6 * n + w];
     c.vse = corners[7 * n + w];
-    const evp::Geom g = evp::make_geom(geo[0 * n + w], geo[1 * n + w], geo[2 * n + w],
+    const evp::Geom g = evp::make_geom_fw(geo[0 * n + w], geo[1 * n + w], geo[2 * n + w],
                                        geo[3 * n + w], geo[4 * n + w], geo[5 * n + w],
                                        p.deltaminEVP);
     double lo[8], ls[12], lc[8], l;
