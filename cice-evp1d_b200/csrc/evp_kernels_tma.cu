@@ -505,16 +505,49 @@ __global__ void __launch_bounds__(kThreads, 1) k_tma(TmaArgs a, Params p) {
         } else {
           // state written by other CTAs in this launch: loads at L2 (not a
           // copy that an earlier read may have left in this SM's L1)
-          if (gw == 0)
-            for (int x = lane; x < nx; x += 32) st.u[kTileOwned + x] = ld_cg(u_in + rec[kRecUvx + x]);
-          if (gw == kGatherWarps - 1)
-            for (int x = lane; x < nx; x += 32) st.v[kTileOwned + x] = ld_cg(v_in + rec[kRecUvx + x]);
-          for (int h = lane; h < nh; h += 32) {
-            const int g = rec[kRecHalo + h];
-            for (int f = gw; f < kTmaStressFields; f += kGatherWarps)
-              st.hf[f][h] = ld_cg((f < 7 ? a.sg[f] : a.s[from][f - 7]) + g);
-            if (gw == kGatherWarps - 1) st.hmeta[h] = a.meta[g];
+          // Each lane issues a batch of loads before it stores any of them,
+          // so that they overlap instead of taking one L2 round trip each.
+          constexpr int kXPer = kTileUvx / 32;  // extras per lane at most
+          for (int c = 0; c < 2; c++) {
+            if (c == 0 ? gw != 0 : gw != kGatherWarps - 1) continue;
+            const double *src = c == 0 ? u_in : v_in;
+            double *dst = (c == 0 ? st.u : st.v) + kTileOwned;
+            double xv[kXPer];
+#pragma unroll
+            for (int i = 0; i < kXPer; i++) {
+              const int x = lane + 32 * i;
+              xv[i] = x < nx ? ld_cg(src + rec[kRecUvx + x]) : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < kXPer; i++)
+              if (lane + 32 * i < nx) dst[lane + 32 * i] = xv[i];
           }
+          // halo: this warp's fields f = gw (mod kGatherWarps) of every halo
+          // point, spread over the lanes by (point, field)
+          const int nf = (kTmaStressFields - gw + kGatherWarps - 1) / kGatherWarps;
+          const int items = nh * nf;
+          constexpr int kBatch = 8;
+          for (int j0 = 0; j0 < items; j0 += 32 * kBatch) {
+            double hv[kBatch];
+#pragma unroll
+            for (int i = 0; i < kBatch; i++) {
+              const int j = j0 + lane + 32 * i;
+              if (j < items) {
+                const int h = j / nf, f = gw + kGatherWarps * (j - h * nf);
+                hv[i] = ld_cg((f < 7 ? a.sg[f] : a.s[from][f - 7]) + rec[kRecHalo + h]);
+              }
+            }
+#pragma unroll
+            for (int i = 0; i < kBatch; i++) {
+              const int j = j0 + lane + 32 * i;
+              if (j < items) {
+                const int h = j / nf, f = gw + kGatherWarps * (j - h * nf);
+                st.hf[f][h] = hv[i];
+              }
+            }
+          }
+          if (gw == kGatherWarps - 1)
+            for (int h = lane; h < nh; h += 32) st.hmeta[h] = a.meta[rec[kRecHalo + h]];
           mbar_arrive(&S.sfull[s]);
         }
         if (gw == 0 && lane == 0) trace_stamp(a, issued, 7);
