@@ -425,6 +425,20 @@ def test_launch_modes_bitwise(oracle_mod, monkeypatch, persist, pdl, ndte):
     assert_same(gpu_run(pr, ndte, calls=1), oracle_run(oracle_mod, pr, ndte), pr)
 
 
+@pytest.mark.parametrize("strip_w,runs", [(64, 3), (48, 148), (8, 20)])
+def test_multi_subcycle_launch_halo_gathers(oracle_mod, monkeypatch, strip_w, runs):
+    """The multi-subcycle launch gathers the forward halo and the extra
+    velocities with coherent loads, each gather lane issuing a batch before it
+    stores any: wide strips (a run's first tile recomputes a whole row above
+    it, up to 64 halo points, several batches per lane) and narrow ones (many
+    halo points in every tile), the same bits as the oracle."""
+    monkeypatch.setenv("EVP1D_PERSIST", "1")
+    monkeypatch.setenv("EVP1D_STRIP_W", str(strip_w))
+    monkeypatch.setenv("EVP1D_RUNS", str(runs))
+    pr = synth.to_1d(synth.make_grid(131, 77, seed=9, ndte=9, curvilinear=True))
+    assert_same(gpu_run(pr, 9, calls=1), oracle_run(oracle_mod, pr, 9), pr)
+
+
 def test_tile_size_tuner():
     """evp1d.tune_tile_points times each candidate on the caller's problem
     (single and batched) and leaves the fastest set."""
