@@ -385,7 +385,11 @@ int evp1d_plan_check(int na, int navel, const int32_t *ee, const int32_t *ne,
  *      uvel_init, vvel_init (only when the recorded call passed them; when
  *      it did not, their gradient is part of uvel, vvel and these are 0).
  * Derivatives take the branch the forward took at max(Delta, DminArea) and
- * are 0 at a zero-length square root.  The recorded forward is dropped by the
+ * are 0 at a zero-length square root.  They are computed in FP64 with fused
+ * multiply-adds (they are not bit-matched to anything; the values that pick
+ * a branch are recomputed with the forward's own rounding), so the same
+ * recording and seed give the same bits on every sweep, and a batched member
+ * the bits of the member solved alone.  The recorded forward is dropped by the
  * next evp1d_upload or evp1d_set_params; one recording can be swept any
  * number of times with different seeds.  Works on batched handles (gradients
  * per member in the member-major [na] layout).
