@@ -126,7 +126,8 @@ def test_memory_sized_recording_with_a_small_budget():
     the full tape: the first subcycles are checkpointed and recomputed, the
     final ones taped; the forward outputs and the gradients are those of the
     full tape, bit for bit, and a second sweep of the same recording (whose
-    segment recompute must not overwrite the taped tail) gives them again."""
+    segment recompute must not overwrite the taped tail) gives them again.
+    The least recording (checkpoints only) gives the same gradients too."""
     pr = small(seed=46, ndte=60)
     uobs, vobs = synth.observations(pr.na, seed=4)
     ga, fa, ia = gpu_grads(pr, pr.ndte, uobs, vobs, interval=0)
@@ -134,9 +135,15 @@ def test_memory_sized_recording_with_a_small_budget():
     full = ia["store_bytes"]
     with evp1d.EVP1D.from_problem(pr) as s:
         s.set_adjoint_budget(1)  # below the minimum: gets the minimum
-        s.run_checkpointed(pr.ndte, evp1d.FieldSet.from_problem(pr), 0)
+        fl = evp1d.FieldSet.from_problem(pr)
+        s.run_checkpointed(pr.ndte, fl, 0)
         least = s.adjoint_info()
+        # every segment recomputed; only the last one's end state is not
+        # stored already (no taped tail), so it alone is recomputed in full
+        gl = s.adjoint(2 * (fl.uvel[: pr.na] - uobs), 2 * (fl.vvel[: pr.na] - vobs))
     assert least["tape_subcycles"] == 0 and least["checkpoints"] > 0, least
+    for k in ga:
+        assert np.array_equal(ga[k].view(np.int64), gl[k].view(np.int64)), k
     budget = (least["store_bytes"] + full) // 2
     fs = evp1d.FieldSet.from_problem(pr)
     with evp1d.EVP1D.from_problem(pr) as s:
