@@ -448,11 +448,10 @@ int evp1d_adjoint_info(evp1d_t *handle, long long info[8]);
  *   host threads, or on streams that run concurrently) race; serialise them.
  * - Every call looks up the array's device address in the current context
  *   (a lookup that allocates nothing), so a cudaDeviceReset or a context of
- *   the caller's own between calls is safe.  The call synchronises
- *   `stream` (it reads the index check back), so it cannot be captured
- *   into a CUDA graph.
+ *   the caller's own between calls is safe.
  * - Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
- *   stream) and the call returns after the stream has finished it.
+ *   stream) and the call returns after the stream has finished it (it reads
+ *   the index check back).
  *   Neighbours outside 1..navel give EVP1D_ERR_INDEX before any array is
  *   written.
  * -------------------------------------------------------------------------- */
