@@ -238,3 +238,20 @@ def test_the_checker_rejects_a_wrong_binding(tmp_path, monkeypatch):
     p.write_text(bad2)
     with pytest.raises(AssertionError, match="evp1d_finalize"):
         test_every_interface_matches_its_c_prototype()
+
+
+def test_integration_examples_use_the_module():
+    """The Fortran snippets of INTEGRATION.md only call procedures the module
+    binds (or defines) and only set fields that evp1d_fields has."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```fortran\n(.*?)```", text, re.S)
+    assert blocks
+    bound = {c.lower() for c in fortran_interfaces()} | {"evp1d_last_error_f"}
+    fields = {f[0] for f in fortran_types()["evp1d_fields"]}
+    for b in blocks:
+        for name in re.findall(r"\b(evp1d_\w+)\s*\(", b):
+            if re.search(r"(function|subroutine)\s+" + name, b):
+                continue  # an interface written out in the snippet itself
+            assert name.lower() in bound, f"INTEGRATION.md calls {name}, which the module does not bind"
+        for f in re.findall(r"\bio%(\w+)", b):
+            assert f.lower() in fields, f"INTEGRATION.md sets io%{f}, not a field of evp1d_fields"
